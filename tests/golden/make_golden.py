@@ -1,0 +1,224 @@
+"""Generate golden fixtures by running the UNMODIFIED TopoGPU reference.
+
+Run in the build container (where the reference source is mounted):
+
+    python tests/golden/make_golden.py /path/to/TopoGPU
+
+The reference's CuPy calls are served by the NumPy-backed stand-in in
+``tests/golden/_cupy_standin`` (CuPy itself is not installed). Outputs are
+small ``.npz`` files next to this script; the GPU box never needs the
+reference. Every array is produced by reference code paths:
+
+  ke_edof.npz      KE_UNIT_3D, _edof_table_3d            (pub_simp_solver.py:157-207)
+  bc.npz           generate_bc on gallery cantilevers    (bc_generator.py:381-447)
+  matvec.npz       MatrixFreeKff.matvec / extract_diagonal (solver_v2.py:1183-1252)
+  transfer.npz     _build_scalar_prolongation, _coarse_free_dofs_injection
+  galerkin.npz     GalerkinMatFreeGMG.setup: K1 (level-1 Galerkin), K2, K3 (R.A.P),
+                   lambda estimates, one V-cycle apply    (multigrid_v4.py)
+  krylov.npz       _cupy_pcg and _cupy_fgmres with the GMG preconditioner
+  solverv4.npz     SolverV4 + topogpu._oc_update, 3 SIMP iterations, config-0
+                   cantilever (FP64 and FP32 smoothers)
+  oc.npz           topogpu.solver._oc_update on seeded inputs
+  filter.npz       _build_density_filter (rmin 1.5, 2.0), DensityFilter.matrix
+  run_simp.npz     run_simp config 0 (rmin 1.5, move 0.2, no Heaviside)
+"""
+
+from __future__ import annotations
+
+import io
+import sys
+from contextlib import redirect_stdout
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+
+
+def _setup(ref_root: Path) -> None:
+    sys.path.insert(0, str(HERE / "_cupy_standin"))
+    sys.path.insert(0, str(ref_root / "src"))
+    sys.path.insert(0, str(ref_root))
+
+
+def _csr(prefix: str, M) -> dict:
+    M = M.tocsr()
+    M.sort_indices()
+    return {f"{prefix}_indptr": M.indptr.astype(np.int64), f"{prefix}_indices": M.indices.astype(np.int64),
+            f"{prefix}_data": np.asarray(M.data, dtype=np.float64), f"{prefix}_shape": np.array(M.shape)}
+
+
+def cantilever_bc(nel):
+    nelx, nely, nelz = nel
+    nny, nnz = nely + 1, nelz + 1
+    ndof = 3 * (nelx + 1) * nny * nnz
+    face = np.arange(nny * nnz)
+    fixed = np.sort(np.concatenate([3 * face, 3 * face + 1, 3 * face + 2]))
+    free = np.setdiff1d(np.arange(ndof), fixed)
+    F = np.zeros(ndof)
+    edge = nelx * nny * nnz + np.arange(nny) * nnz
+    F[3 * edge + 2] = -1.0 / len(edge)
+    return fixed, free, F, ndof
+
+
+def main(ref_root: str) -> None:
+    _setup(Path(ref_root))
+    import gpu_fem.multigrid_v4 as mg
+    import gpu_fem.solver_v2 as sv2
+    from gpu_fem.bc_generator import generate_bc
+    from gpu_fem.pub_simp_solver import (KE_UNIT_3D, SIMPParams, _build_density_filter,
+                                         _edof_table_3d, run_simp)
+    from gpu_fem.solver_v4 import SolverV4
+    import topogpu as tg
+    from topogpu.solver import _oc_update
+
+    import cupy as cp
+
+    out = {}
+    # ---- KE / edof ------------------------------------------------------
+    np.savez_compressed(HERE / "ke_edof.npz", KE=KE_UNIT_3D, edof_432=_edof_table_3d(4, 3, 2),
+                        edof_753=_edof_table_3d(7, 5, 3))
+
+    # ---- BCs from the public gallery -----------------------------------
+    d = {}
+    for nel in [(4, 3, 2), (24, 12, 6), (7, 5, 3)]:
+        p = tg.gallery.cantilever_3d(nel=nel, volfrac=0.3)
+        bc = generate_bc(p.spec)
+        tag = "x".join(map(str, nel))
+        d[f"free_{tag}"] = bc.free_dofs.astype(np.int64)
+        d[f"F_{tag}"] = bc.F
+        p2 = tg.gallery.side_load_cantilever(nel=nel)
+        bc2 = generate_bc(p2.spec)
+        d[f"side_free_{tag}"] = bc2.free_dofs.astype(np.int64)
+        d[f"side_F_{tag}"] = bc2.F
+    np.savez_compressed(HERE / "bc.npz", **d)
+
+    # ---- matvec / diagonal ---------------------------------------------
+    d = {}
+    for nel in [(24, 12, 6), (7, 5, 3)]:
+        tag = "x".join(map(str, nel))
+        edof = _edof_table_3d(*nel)
+        fixed, free, F, ndof = cantilever_bc(nel)
+        rng = np.random.default_rng(7)
+        rho = rng.uniform(0.001, 1.0, edof.shape[0])
+        E = 1e-9 + (1 - 1e-9) * rho**3
+        u = rng.standard_normal(len(free))
+        op = sv2.MatrixFreeKff(cp.asarray(edof), cp.asarray(KE_UNIT_3D), cp.asarray(free.astype(np.int32)),
+                               len(free), ndof)
+        d[f"rho_{tag}"] = rho
+        d[f"u_{tag}"] = u
+        d[f"y64_{tag}"] = np.asarray(op.matvec(cp.asarray(u), cp.asarray(E)))
+        d[f"y32_{tag}"] = np.asarray(op.matvec(cp.asarray(u.astype(np.float32)), cp.asarray(E.astype(np.float32))))
+        d[f"diag_{tag}"] = np.asarray(op.extract_diagonal(cp.asarray(E)))
+    np.savez_compressed(HERE / "matvec.npz", **d)
+
+    # ---- transfers ------------------------------------------------------
+    d = {}
+    pairs = [((24, 12, 6), (12, 6, 3)), ((12, 6, 3), (6, 3, 1)), ((6, 3, 1), (3, 1, 1)),
+             ((7, 5, 3), (3, 2, 1)), ((3, 2, 1), (1, 1, 1)), ((1, 1, 1), (1, 1, 1))]
+    for fine, coarse in pairs:
+        tag = "x".join(map(str, fine)) + "_" + "x".join(map(str, coarse))
+        d.update(_csr(f"P_{tag}", sv2._build_scalar_prolongation(*fine, *coarse)))
+        fixed, free, F, ndof = cantilever_bc(fine)
+        d[f"inj_{tag}"] = sv2._coarse_free_dofs_injection(*fine, *coarse, free).astype(np.int64)
+    np.savez_compressed(HERE / "transfer.npz", **d)
+
+    # ---- GMG setup / apply ---------------------------------------------
+    d = {}
+    for nel, nlev in [((24, 12, 6), 4), ((7, 5, 3), 3)]:
+        tag = "x".join(map(str, nel))
+        edof = _edof_table_3d(*nel)
+        fixed, free, F, ndof = cantilever_bc(nel)
+        rng = np.random.default_rng(11)
+        rho = rng.uniform(0.05, 1.0, edof.shape[0])
+        E = 1e-9 + (1 - 1e-9) * rho**3
+        free_gpu = cp.asarray(free.astype(np.int32))
+        op = sv2.MatrixFreeKff(cp.asarray(edof), cp.asarray(KE_UNIT_3D), free_gpu, len(free), ndof)
+        with redirect_stdout(io.StringIO()):
+            g = mg.GalerkinMatFreeGMG(mf_op=op, free=free.astype(np.int32), free_gpu=free_gpu, nelx=nel[0],
+                                      nely=nel[1], nelz=nel[2], KE_UNIT=KE_UNIT_3D, n_levels=nlev,
+                                      fine_smoother="fp64", fine_smoother_degree=2)
+            g.setup(cp.asarray(E))
+        d[f"rho_{tag}"] = rho
+        for lv in range(1, nlev):
+            d.update(_csr(f"K{lv}_{tag}", g._K_gpu[lv]))
+            d[f"free{lv}_{tag}"] = np.asarray(g._free_per_level[lv]).astype(np.int64)
+        d[f"lam_{tag}"] = np.array(g._lambda_max_per_level)
+        r = rng.standard_normal(len(free))
+        d[f"r_{tag}"] = r
+        d[f"z_{tag}"] = np.asarray(g.apply(cp.asarray(r)))
+        d[f"chol_mode_{tag}"] = np.array(g._coarse_chol_mode)
+        # krylov on this hierarchy
+        Fd = cp.asarray(F[free])
+        x, it, ok = sv2._cupy_pcg(lambda v: op.matvec(v, cp.asarray(E)), Fd, g.apply, tol=1e-8, maxiter=500)
+        d[f"pcg_x_{tag}"] = np.asarray(x)
+        d[f"pcg_it_{tag}"] = np.array(it)
+        x2, it2, ok2 = mg._cupy_fgmres(lambda v: op.matvec(v, cp.asarray(E)), Fd, g.apply, tol=1e-8,
+                                       maxiter=500, restart=32)
+        d[f"fgmres_x_{tag}"] = np.asarray(x2)
+        d[f"fgmres_it_{tag}"] = np.array(it2)
+    np.savez_compressed(HERE / "galerkin.npz", **d)
+
+    # ---- SolverV4 + OC, config-0 cantilever ------------------------------
+    d = {}
+    nel = (24, 12, 6)
+    edof = _edof_table_3d(*nel)
+    fixed, free, F, ndof = cantilever_bc(nel)
+    for prec in ["fp64", "fp32"]:
+        with redirect_stdout(io.StringIO()):
+            s = SolverV4(edof=edof, row_idx=None, col_idx=None, KE_UNIT=KE_UNIT_3D, free=free.astype(np.int32),
+                         F=F, ndof=ndof, backend="cupy", enable_warm_start=True, enable_matrix_free=True,
+                         enable_fused_cuda=False, enable_matfree_gmg=True, matfree_gmg_levels=4,
+                         gmg_fine_smoother=prec, gmg_smoother_type="chebyshev", grid_dims=nel, cg_tol=1e-8,
+                         cg_maxiter=800, enable_profiling=True)
+            rho = np.full(edof.shape[0], 0.3)
+            comps, iters, rhos, dcs = [], [], [], []
+            for _ in range(3):
+                c, dc = s.solve(rho, penal=3.0)
+                comps.append(c)
+                iters.append(s.last_cg_iters)
+                dcs.append(dc)
+                rho = _oc_update(rho, dc, 0.3, 0.2, 1e-3)
+                rhos.append(rho)
+        d[f"compliance_{prec}"] = np.array(comps)
+        d[f"iters_{prec}"] = np.array(iters)
+        d[f"rho_{prec}"] = np.stack(rhos)
+        d[f"dc_{prec}"] = np.stack(dcs)
+    np.savez_compressed(HERE / "solverv4.npz", **d)
+
+    # ---- OC on seeded inputs ----------------------------------------------
+    d = {}
+    rng = np.random.default_rng(3)
+    for k, (n, vf, mv) in enumerate([(1728, 0.3, 0.2), (5000, 0.25, 0.1), (64, 0.5, 0.05)]):
+        rho = rng.uniform(0.001, 1.0, n)
+        dc = -rng.gamma(1.0, 1.0, n) * 10.0 ** rng.uniform(-6, 1, n)
+        dc[::17] = 0.0  # exercises the min(dc, -1e-12) guard
+        d[f"rho_{k}"] = rho
+        d[f"dc_{k}"] = dc
+        d[f"vf_{k}"] = np.array(vf)
+        d[f"move_{k}"] = np.array(mv)
+        d[f"out_{k}"] = _oc_update(rho, dc, vf, mv, 1e-3)
+    np.savez_compressed(HERE / "oc.npz", **d)
+
+    # ---- filters -----------------------------------------------------------
+    d = {}
+    for nel, rmin in [((24, 12, 6), 1.5), ((7, 5, 3), 2.0), ((6, 4, 3), 2.3)]:
+        tag = "x".join(map(str, nel)) + f"_r{rmin}"
+        d.update(_csr(f"H_{tag}", _build_density_filter(nel[0], nel[1], rmin, nel[2])))
+    d["dense_432_r1.5"] = tg.DensityFilter((4, 3, 2), radius=1.5).matrix()
+    d["dense_322_r1.5"] = tg.DensityFilter((3, 2, 2), radius=1.5).matrix()
+    np.savez_compressed(HERE / "filter.npz", **d)
+
+    # ---- run_simp config 0 ---------------------------------------------------
+    nel = (24, 12, 6)
+    fixed, free, F, ndof = cantilever_bc(nel)
+    params = SIMPParams(nelx=24, nely=12, nelz=6, volfrac=0.3, rmin=1.5, move=0.2, max_iter=3, min_iter=3,
+                        use_heaviside=False)
+    res = run_simp(params, verbose=False, bc_override=lambda a, b, c: (fixed, free, F))
+    np.savez_compressed(HERE / "run_simp.npz", compliance=np.array(res["compliance_history"]),
+                        final=np.array(res["final_compliance"]), rho_final=res["rho_final"])
+    print("golden fixtures written to", HERE)
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
