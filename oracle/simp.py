@@ -65,6 +65,28 @@ def simp_solverv4(nel, bc, volfrac, max_iter, move=0.10, rho_min=1e-3, **kw):
     return rho, comp, rhos
 
 
+class FilteredSIMP:
+    """run_simp-style filtered SIMP whose state solve is the SolverV4 GMG-PCG
+    restatement (the reference's GPU algorithm run on the host): one
+    ``step()`` = filter, state solve, sensitivity, H^T chain, filtered OC.
+    Used as the timed CPU baseline."""
+
+    def __init__(self, nel, bc, volfrac, rmin, move=0.2, penal=3.0, **solver_kw):
+        self.nel, self.bc = tuple(nel), bc
+        self.H = design.filter_matrix(nel, rmin)
+        n = self.H.shape[0]
+        self.rho = np.full(n, float(volfrac))
+        self.dv = self.H.T @ np.ones(n)
+        self.volfrac, self.move, self.penal = volfrac, move, penal
+        self.state = StateSolverV4(nel, bc, **solver_kw)
+
+    def step(self):
+        rp = self.H @ self.rho
+        c, dc = self.state.solve(rp, self.penal)
+        self.rho, _ = design.oc_update_filtered(self.rho, self.H.T @ dc, self.dv, self.volfrac, self.move, self.H)
+        return c
+
+
 def simp_filtered(nel, bc, volfrac, rmin, max_iter, move=0.2, penal=3.0, solve=None):
     """``run_simp`` main loop without Heaviside, callbacks or tail
     (pub_simp_solver.py:412-657, _fea_and_sensitivity 342-377): physical

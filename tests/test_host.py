@@ -1,0 +1,123 @@
+"""Host-side logic and the C ABI library, without a GPU."""
+
+from __future__ import annotations
+
+import csv
+import ctypes
+import re
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, load_golden
+
+
+def test_library_loads_and_exports_every_declared_symbol():
+    from topogpu_b200 import _lib, build
+
+    build.build()
+    lib = _lib.load()
+    header = (ROOT / "include" / "topo_b200.h").read_text()
+    declared = set(re.findall(r"^\s*(?:int|long long)\s+(topo_\w+)\s*\(", header, flags=re.M))
+    assert declared, "no declarations found in include/topo_b200.h"
+    for name in declared:
+        assert hasattr(lib, name), name
+    assert declared <= set(_lib.SIGNATURES), declared - set(_lib.SIGNATURES)
+    assert lib.topo_version() == 100
+
+
+def test_library_reports_errors_without_gpu_work():
+    from topogpu_b200 import _lib
+
+    lib = _lib.load()
+    h = ctypes.c_void_p()
+    ke = np.zeros(576)
+    rc = lib.topo_ctx_create(0, 1, 1, 1, 0, 2, 2, 1 / 30, 100, ke.ctypes.data_as(ctypes.c_void_p), ctypes.byref(h))
+    assert rc < 0
+    assert "grid dims" in _lib.last_error(None)
+
+
+def test_product_stiffness_matches_reference():
+    from topogpu_b200.fem import KE_UNIT
+
+    np.testing.assert_allclose(KE_UNIT, load_golden("ke_edof")["KE"], rtol=0, atol=1e-14)
+
+
+@pytest.mark.parametrize("tag,nel", [("4x3x2", (4, 3, 2)), ("24x12x6", (24, 12, 6)), ("7x5x3", (7, 5, 3))])
+def test_generate_bc_matches_reference(tag, nel):
+    import topogpu_b200 as tg
+    from topogpu_b200.bc import generate_bc
+
+    g = load_golden("bc")
+    bc = generate_bc(tg.gallery.cantilever_3d(nel=nel, volfrac=0.3).spec)
+    assert np.array_equal(bc.free_dofs, g[f"free_{tag}"])
+    assert np.array_equal(bc.F, g[f"F_{tag}"])
+    bc2 = generate_bc(tg.gallery.side_load_cantilever(nel=nel).spec)
+    assert np.array_equal(bc2.free_dofs, g[f"side_free_{tag}"])
+    assert np.array_equal(bc2.F, g[f"side_F_{tag}"])
+
+
+def test_problem_validation_errors():
+    import topogpu_b200 as tg
+
+    p = tg.gallery.cantilever_3d(nel=(4, 3, 2), volfrac=0.30)
+    p.validate()
+    assert p.nel == (4, 3, 2) and p.volfrac == 0.30 and p.metadata["support"] == "xmin"
+    p.spec.volfrac = 2.0
+    with pytest.raises(ValueError, match="Volume fraction"):
+        p.validate()
+    with pytest.raises(ValueError):
+        tg.gallery.cantilever_3d(support="ymin")
+
+
+def test_spec_round_trip():
+    import topogpu_b200 as tg
+    from topogpu_b200.problem_spec import ProblemSpec
+
+    spec = tg.gallery.cantilever_3d().spec
+    assert ProblemSpec.from_dict(spec.to_dict()).to_dict() == spec.to_dict()
+
+
+def test_density_filter_host_api():
+    import topogpu_b200 as tg
+
+    f = tg.DensityFilter((4, 3, 2), radius=1.5)
+    assert np.allclose(f.apply(np.ones(24)), 1.0, atol=1e-12)
+    np.testing.assert_allclose(tg.DensityFilter((4, 3, 2), 1.5).matrix(), load_golden("filter")["dense_432_r1.5"],
+                               rtol=1e-15)
+    w = tg.DensityFilter((3, 2, 2), radius=1.5).matrix()
+    assert np.allclose(w.sum(axis=1), 1.0, atol=1e-12)
+
+
+def test_evidence_bundle_manifest(tmp_path):
+    from topogpu_b200.evidence import EvidenceBundle
+
+    b = EvidenceBundle(tmp_path)
+    b.write_history([{"iteration": 1, "compliance": 1.0}, {"iteration": 2, "compliance": 0.5, "wall_s": 0.1}])
+    b.write_summary({"status": "ok"})
+    b.write_density(np.ones(3))
+    b.write_render_metadata({"density_threshold": 0.5})
+    m = b.write_manifest()
+    rows = list(csv.DictReader(m.open()))
+    assert {r["path"] for r in rows} >= {"history.csv", "summary.json", "rho_final.npy", "render_metadata.json"}
+    assert all(len(r["sha256"]) == 64 for r in rows)
+    head = (tmp_path / "history.csv").read_text().splitlines()[0]
+    assert head == "compliance,iteration,wall_s"
+
+
+def test_cpu_backend_is_rejected_loudly():
+    import topogpu_b200 as tg
+
+    with pytest.raises(ValueError, match="GPU-only"):
+        tg.SIMPSolver(backend="cpu")
+    with pytest.raises(ValueError, match="optimizer"):
+        tg.SIMPSolver(optimizer="mma")
+
+
+def test_benchmark_problem_load():
+    import topogpu_b200 as tg
+
+    p = tg.gallery.benchmark_cantilever((24, 12, 6))
+    F = p.force_override
+    assert abs(F.sum() + 1.0) < 1e-14 and np.count_nonzero(F) == 13

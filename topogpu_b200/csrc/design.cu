@@ -1,0 +1,336 @@
+// design.cu - density filter, OC updates and field statistics on the device.
+//
+// The OC bisection keeps its whole state (lambda bracket, phase, counters) in
+// device memory: each pass evaluates one candidate's volume with a
+// deterministic grid reduction and the last block advances the bisection, so
+// the host only checks a "done" flag every few passes instead of reading a
+// mean per step (the reference runs the loop in NumPy on the host,
+// src/topogpu/solver.py:94-117).
+#include "internal.cuh"
+#include "reduce.cuh"
+
+#include <cmath>
+#include <functional>
+#include <stdexcept>
+#include <vector>
+
+namespace topo {
+
+constexpr int kMaxFilterOff = 1331;  // (2*5+1)^3: rmin < 6
+__constant__ int cFoff[kMaxFilterOff][3];
+__constant__ double cFw[kMaxFilterOff];
+
+struct FilterStencil {
+  double rmin = -1.0;
+  int n = 0;
+};
+static FilterStencil g_filter;
+
+// Offsets and weights of the linear-hat filter: every element at centre
+// distance d <= rmin - 1e-10 with weight rmin - d, plus the element itself with
+// weight rmin (pub_simp_solver.py:215-243; kd-tree query_pairs radius).
+static void set_filter(double rmin, cudaStream_t s) {
+  if (g_filter.rmin == rmin) return;
+  const int R = (int)std::floor(rmin);
+  std::vector<int> off;
+  std::vector<double> w;
+  for (int dx = -R; dx <= R; ++dx)
+    for (int dy = -R; dy <= R; ++dy)
+      for (int dz = -R; dz <= R; ++dz) {
+        const double d = std::sqrt((double)(dx * dx + dy * dy + dz * dz));
+        if (dx == 0 && dy == 0 && dz == 0) {
+          off.insert(off.end(), {0, 0, 0});
+          w.push_back(rmin);
+        } else if (d <= rmin - 1e-10) {
+          off.insert(off.end(), {dx, dy, dz});
+          w.push_back(rmin - d);
+        }
+      }
+  if ((int)w.size() > kMaxFilterOff) throw std::runtime_error("filter radius too large (rmin must be < 6)");
+  TOPO_CUDA_CHECK(cudaMemcpyToSymbolAsync(cFoff, off.data(), sizeof(int) * off.size(), 0, cudaMemcpyHostToDevice, s));
+  TOPO_CUDA_CHECK(cudaMemcpyToSymbolAsync(cFw, w.data(), sizeof(double) * w.size(), 0, cudaMemcpyHostToDevice, s));
+  TOPO_CUDA_CHECK(cudaStreamSynchronize(s));
+  g_filter.rmin = rmin;
+  g_filter.n = (int)w.size();
+}
+
+__device__ __forceinline__ double row_weight_sum(const Grid& g, int ex, int ey, int ez, int noff) {
+  double hs = 0.0;
+  for (int k = 0; k < noff; ++k) {
+    const int x = ex + cFoff[k][0], y = ey + cFoff[k][1], z = ez + cFoff[k][2];
+    if (x >= 0 && x < g.nx && y >= 0 && y < g.ny && z >= 0 && z < g.nz) hs += cFw[k];
+  }
+  return hs;
+}
+
+__global__ void k_filter_rowsum(Grid g, int noff, double* __restrict__ Hs) {
+  const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (e >= g.nelem) return;
+  const int ez = e % g.nz, ey = (e / g.nz) % g.ny, ex = e / ((long long)g.nz * g.ny);
+  Hs[e] = row_weight_sum(g, ex, ey, ez, noff);
+}
+
+// out_i = sum_j (w_ij / Hs_i) in_j          (transpose = 0)
+// out_j = sum_i (w_ij / Hs_i) in_i          (transpose = 1)
+__global__ void k_filter(Grid g, int noff, const double* __restrict__ in, double* __restrict__ out,
+                         const double* __restrict__ Hs, int transpose) {
+  const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (e >= g.nelem) return;
+  const int ez = e % g.nz, ey = (e / g.nz) % g.ny, ex = e / ((long long)g.nz * g.ny);
+  double acc = 0.0;
+  if (!transpose) {
+    const double hs = Hs[e];
+    for (int k = 0; k < noff; ++k) {
+      const int x = ex + cFoff[k][0], y = ey + cFoff[k][1], z = ez + cFoff[k][2];
+      if (x < 0 || x >= g.nx || y < 0 || y >= g.ny || z < 0 || z >= g.nz) continue;
+      acc += (cFw[k] / hs) * in[((long long)x * g.ny + y) * g.nz + z];
+    }
+  } else {
+    for (int k = 0; k < noff; ++k) {
+      const int x = ex + cFoff[k][0], y = ey + cFoff[k][1], z = ez + cFoff[k][2];
+      if (x < 0 || x >= g.nx || y < 0 || y >= g.ny || z < 0 || z >= g.nz) continue;
+      const long long i = ((long long)x * g.ny + y) * g.nz + z;
+      acc += (cFw[k] / Hs[i]) * in[i];
+    }
+  }
+  out[e] = acc;
+}
+
+void filter_apply(const Grid& g, double rmin, const double* in, double* out, bool transpose, double* Hs_work,
+                  cudaStream_t s) {
+  set_filter(rmin, s);
+  const int bs = 256;
+  const unsigned nb = (unsigned)((g.nelem + bs - 1) / bs);
+  k_filter_rowsum<<<nb, bs, 0, s>>>(g, g_filter.n, Hs_work);
+  TOPO_LAUNCH_CHECK();
+  k_filter<<<nb, bs, 0, s>>>(g, g_filter.n, in, out, Hs_work, transpose ? 1 : 0);
+  TOPO_LAUNCH_CHECK();
+}
+
+// ------------------------------------------------------------------- OC
+// Device state of the bisection. Slots of a double[16] array:
+enum OcSlot { OC_LO = 0, OC_HI, OC_EVAL, OC_MID, OC_MEAN, OC_PHASE, OC_NBIS, OC_DONE, OC_EVALS };
+
+__device__ __forceinline__ double oc_candidate(double rho, double dc, double lam, double move, double rho_min) {
+  const double dcs = fmin(dc, -1.0e-12);
+  double t = -dcs / fmax(lam, 1.0e-40);
+  t = fmax(t, 0.0);
+  const double v = rho * sqrt(t);
+  const double lo = fmax(rho - move, rho_min);
+  const double hi = fmin(rho + move, 1.0);
+  return fmin(fmax(v, lo), hi);
+}
+
+__global__ void k_oc_pass(long long n, const double* __restrict__ rho, const double* __restrict__ dc,
+                          double volfrac, double move, double rho_min, double* st, RedWork red) {
+  if (st[OC_DONE] != 0.0) return;
+  const double lam = st[OC_EVAL];
+  double v[1] = {0.0};
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    v[0] += oc_candidate(rho[i], dc[i], lam, move, rho_min);
+  double tot[1];
+  if (grid_sum<1>(v, red, tot) && threadIdx.x == 0) {
+    const double mean = tot[0] / (double)n;
+    st[OC_MEAN] = mean;
+    st[OC_EVALS] += 1.0;
+    if (st[OC_PHASE] == 0.0) {
+      // lambda_hi doubling while the candidate volume is too large
+      if (mean > volfrac && st[OC_HI] < 1.0e40) {
+        st[OC_LO] = st[OC_HI];
+        st[OC_HI] = st[OC_HI] * 2.0;
+        st[OC_EVAL] = st[OC_HI];
+      } else {
+        st[OC_PHASE] = 1.0;
+        st[OC_EVAL] = 0.5 * (st[OC_LO] + st[OC_HI]);
+      }
+    } else {
+      const double mid = st[OC_EVAL];
+      if (mean > volfrac) st[OC_LO] = mid;
+      else st[OC_HI] = mid;
+      st[OC_MID] = mid;
+      st[OC_NBIS] += 1.0;
+      if (fabs(mean - volfrac) < 1.0e-8 || st[OC_NBIS] >= 80.0) st[OC_DONE] = 1.0;
+      else st[OC_EVAL] = 0.5 * (st[OC_LO] + st[OC_HI]);
+    }
+  }
+}
+
+__global__ void k_oc_final(long long n, const double* __restrict__ rho, const double* __restrict__ dc, double move,
+                           double rho_min, const double* st, double* __restrict__ out) {
+  const double lam = st[OC_MID];
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    out[i] = oc_candidate(rho[i], dc[i], lam, move, rho_min);
+}
+
+__global__ void k_oc_init(double* st) {
+  for (int i = 0; i < 16; ++i) st[i] = 0.0;
+  st[OC_LO] = 0.0;
+  st[OC_HI] = 1.0;
+  st[OC_EVAL] = 1.0;
+}
+
+static int run_until_done(const std::function<void()>& pass, const double* st, int max_passes, cudaStream_t s) {
+  double h[16];
+  int launched = 0;
+  while (launched < max_passes) {
+    const int chunk = launched < 16 ? 8 : 16;
+    for (int k = 0; k < chunk && launched < max_passes; ++k, ++launched) pass();
+    TOPO_CUDA_CHECK(cudaMemcpyAsync(h, st, sizeof(double) * 16, cudaMemcpyDeviceToHost, s));
+    TOPO_CUDA_CHECK(cudaStreamSynchronize(s));
+    if (h[OC_DONE] != 0.0) return (int)h[OC_EVALS];
+  }
+  return -1;
+}
+
+int oc_update(long long n, const double* rho, const double* dc, double volfrac, double move, double rho_min,
+              double* out, RedWork red, double* st, cudaStream_t s) {
+  k_oc_init<<<1, 1, 0, s>>>(st);
+  TOPO_LAUNCH_CHECK();
+  const unsigned nb = (unsigned)std::min<long long>(kRedBlocks, (n + kRedThreads - 1) / kRedThreads);
+  auto pass = [&]() {
+    k_oc_pass<<<nb, kRedThreads, 0, s>>>(n, rho, dc, volfrac, move, rho_min, st, red);
+    TOPO_LAUNCH_CHECK();
+  };
+  // at most 134 doublings (1 -> 2^133 > 1e40) and 80 bisections
+  const int evals = run_until_done(pass, st, 134 + 80 + 1, s);
+  if (evals < 0) throw std::runtime_error("OC bisection did not terminate");
+  k_oc_final<<<nb, kRedThreads, 0, s>>>(n, rho, dc, move, rho_min, st, out);
+  TOPO_LAUNCH_CHECK();
+  return evals;
+}
+
+// ------------------------------------------------------- filtered-volume OC
+enum OcfSlot { OF_L1 = 0, OF_L2, OF_LM, OF_LAST, OF_K, OF_DONE, OF_EVALS };
+
+__device__ __forceinline__ double ocf_candidate(double rho, double dc, double dv, double lm, double move,
+                                                double rho_min) {
+  const double dcs = fmin(dc, -1e-12);
+  const double dvs = fmax(dv, 1e-12);
+  double rn = rho * sqrt(-dcs / (lm * dvs));
+  rn = fmin(fmax(rn, rho - move), rho + move);
+  rn = fmin(fmax(rn, rho_min), 1.0);
+  return rn;
+}
+
+__global__ void k_ocf_pass(long long n, const double* __restrict__ rho, const double* __restrict__ dc,
+                           const double* __restrict__ dv, const double* __restrict__ colsum, double volfrac,
+                           double move, double rho_min, double* st, RedWork red) {
+  if (st[OF_DONE] != 0.0) return;
+  const double lm = st[OF_LM];
+  double v[1] = {0.0};
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    v[0] += ocf_candidate(rho[i], dc[i], dv[i], lm, move, rho_min) * colsum[i];
+  double tot[1];
+  if (grid_sum<1>(v, red, tot) && threadIdx.x == 0) {
+    st[OF_EVALS] += 1.0;
+    if (tot[0] / (double)n > volfrac) st[OF_L1] = lm;
+    else st[OF_L2] = lm;
+    st[OF_LAST] = lm;
+    st[OF_K] += 1.0;
+    if (st[OF_L2] - st[OF_L1] < 1e-9 || st[OF_K] >= 100.0) st[OF_DONE] = 1.0;
+    else st[OF_LM] = 0.5 * (st[OF_L1] + st[OF_L2]);
+  }
+}
+
+__global__ void k_ocf_init(double* st) {
+  for (int i = 0; i < 16; ++i) st[i] = 0.0;
+  st[OF_L1] = 0.0;
+  st[OF_L2] = 1e9;
+  st[OF_LM] = 0.5 * (0.0 + 1e9);
+}
+
+__global__ void k_ocf_final(long long n, const double* __restrict__ rho, const double* __restrict__ dc,
+                            const double* __restrict__ dv, double move, double rho_min, const double* st,
+                            double* __restrict__ out) {
+  const double lm = st[OF_LAST];
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    out[i] = ocf_candidate(rho[i], dc[i], dv[i], lm, move, rho_min);
+}
+
+int oc_update_filtered(long long n, const double* rho, const double* dc, const double* dv, const double* colsum,
+                       double volfrac, double move, double rho_min, double* out, RedWork red, double* st,
+                       cudaStream_t s) {
+  k_ocf_init<<<1, 1, 0, s>>>(st);
+  TOPO_LAUNCH_CHECK();
+  const unsigned nb = (unsigned)std::min<long long>(kRedBlocks, (n + kRedThreads - 1) / kRedThreads);
+  auto pass = [&]() {
+    k_ocf_pass<<<nb, kRedThreads, 0, s>>>(n, rho, dc, dv, colsum, volfrac, move, rho_min, st, red);
+    TOPO_LAUNCH_CHECK();
+  };
+  double h[16];
+  int launched = 0;
+  while (true) {
+    for (int k = 0; k < 16 && launched < 100; ++k, ++launched) pass();
+    TOPO_CUDA_CHECK(cudaMemcpyAsync(h, st, sizeof(double) * 16, cudaMemcpyDeviceToHost, s));
+    TOPO_CUDA_CHECK(cudaStreamSynchronize(s));
+    if (h[OF_DONE] != 0.0) break;
+    if (launched >= 100) throw std::runtime_error("filtered OC bisection did not terminate");
+  }
+  k_ocf_final<<<nb, kRedThreads, 0, s>>>(n, rho, dc, dv, move, rho_min, st, out);
+  TOPO_LAUNCH_CHECK();
+  return (int)h[OF_EVALS];
+}
+
+// ------------------------------------------------------------ field stats
+__global__ void k_stats(long long n, const double* __restrict__ x, double* out4, RedWork red) {
+  double sum = 0.0, gray = 0.0, mn = INFINITY, mx = -INFINITY;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const double v = x[i];
+    sum += v;
+    gray += v * (1.0 - v);
+    mn = fmin(mn, v);
+    mx = fmax(mx, v);
+  }
+  __shared__ double smn[32], smx[32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  mn = warp_min(mn);
+  mx = warp_max(mx);
+  if (lane == 0) {
+    smn[wid] = mn;
+    smx[wid] = mx;
+  }
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    const int nw = blockDim.x >> 5;
+    mn = warp_min(threadIdx.x < nw ? smn[threadIdx.x] : INFINITY);
+    mx = warp_max(threadIdx.x < nw ? smx[threadIdx.x] : -INFINITY);
+  }
+  // min/max travel through the sum slots of a separate partial row
+  double v[4] = {sum, gray, 0.0, 0.0};
+  __shared__ bool s_last;
+  block_sum<4>(v);
+  const unsigned nb = gridDim.x;
+  if (threadIdx.x == 0) {
+    red.partials[(size_t)blockIdx.x * 4 + 0] = v[0];
+    red.partials[(size_t)blockIdx.x * 4 + 1] = v[1];
+    red.partials[(size_t)blockIdx.x * 4 + 2] = mn;
+    red.partials[(size_t)blockIdx.x * 4 + 3] = mx;
+    __threadfence();
+    s_last = (atomicAdd(red.ticket, 1u) == nb - 1);
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  if (threadIdx.x == 0) {
+    double S = 0.0, G = 0.0, MN = INFINITY, MX = -INFINITY;
+    for (unsigned b = 0; b < nb; ++b) {
+      S += __ldcg(red.partials + (size_t)b * 4 + 0);
+      G += __ldcg(red.partials + (size_t)b * 4 + 1);
+      MN = fmin(MN, __ldcg(red.partials + (size_t)b * 4 + 2));
+      MX = fmax(MX, __ldcg(red.partials + (size_t)b * 4 + 3));
+    }
+    out4[0] = S / (double)n;
+    out4[1] = MN;
+    out4[2] = MX;
+    out4[3] = 4.0 * (G / (double)n);
+    *red.ticket = 0u;
+  }
+}
+
+void field_stats(long long n, const double* x, double* out4_dev, RedWork red, cudaStream_t s) {
+  const unsigned nb = (unsigned)std::min<long long>(kRedBlocks, (n + kRedThreads - 1) / kRedThreads);
+  k_stats<<<nb, kRedThreads, 0, s>>>(n, x, out4_dev, red);
+  TOPO_LAUNCH_CHECK();
+}
+
+}  // namespace topo

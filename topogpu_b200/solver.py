@@ -1,0 +1,187 @@
+"""Public SIMP driver: ``SIMPSolver(backend="cuda", ...).solve(problem)``.
+
+Drop-in for the reference's SolverV4 path (src/topogpu/solver.py:124-253):
+same constructor arguments, same ``OptimizationResult`` and evidence bundle,
+same history/summary keys. Each iteration runs entirely on the GPU: E(rho),
+GMG setup, Krylov solve, compliance, sensitivity and the bisection OC update
+(the reference does the OC in host NumPy); the host only reads the scalars
+that go into the history rows.
+
+Defaults reproduce the reference path: no density filter, penalty 3,
+OC on the plain mean volume. ``use_filter=True`` switches to the filtered
+formulation of the reference's CPU driver ``run_simp``
+(src/gpu_fem/pub_simp_solver.py:342-377): physical density H rho,
+sensitivities chained through H^T, volume measured after the filter.
+"""
+
+from __future__ import annotations
+
+import time
+from dataclasses import dataclass
+from pathlib import Path
+from typing import Any
+
+import numpy as np
+import torch
+
+from .bc import generate_bc
+from .evidence import EvidenceBundle
+from .problem import TopologyProblem
+from .state import StateSolver
+
+
+@dataclass
+class SIMPModel:
+    penal: float = 3.0
+    rho_min: float = 1.0e-3
+
+
+@dataclass
+class OCOptimizer:
+    move: float = 0.10
+
+
+@dataclass
+class OptimizationResult:
+    problem: TopologyProblem
+    rho_final: np.ndarray
+    history: list
+    summary: dict
+
+    def save(self, path) -> EvidenceBundle:
+        bundle = EvidenceBundle(Path(path))
+        bundle.write_history(self.history)
+        bundle.write_density(self.rho_final)
+        bundle.write_render_metadata({"density_threshold": 0.5, "scalar": "density",
+                                      "scalar_normalization": "per_case_0_1", "camera": "orthographic_default",
+                                      "source": "OptimizationResult.save"})
+        bundle.write_summary(self.summary)
+        bundle.write_manifest()
+        return bundle
+
+
+_PRECISIONS = ("fp64", "fp32", "mixed")
+
+
+class SIMPSolver:
+    """Bounded SIMP loop on one B200.
+
+    Reference arguments: backend, linear_solver, optimizer, tol, max_krylov,
+    max_iter, move, rho_min. Extra (optional) arguments: precision
+    ("mixed" default, "fp32", "fp64"), levels, fine_degree, coarse_degree,
+    use_filter, penal, smoother ("chebyshev" default, "reference"), device.
+    """
+
+    def __init__(self, backend="cuda", linear_solver="auto", optimizer="oc", tol=1.0e-5, max_krylov=800,
+                 max_iter=12, move=0.10, rho_min=1.0e-3, *, precision="mixed", levels=4, fine_degree=2,
+                 coarse_degree=2, use_filter=False, penal=3.0, smoother="chebyshev", device=None):
+        if optimizer != "oc":
+            raise ValueError("Only optimizer='oc' is implemented in v0.1.0.")
+        if backend in {"cpu", "scipy"}:
+            raise ValueError("backend='cpu' is not part of topogpu_b200 (GPU-only build); use backend='cuda'.")
+        if backend not in {"cuda", "cupy"}:
+            raise ValueError(f"Unknown backend {backend!r}.")
+        if linear_solver not in {"auto", "pcg_gmg", "fgmres_gmg"}:
+            raise ValueError(f"Unknown linear_solver {linear_solver!r}.")
+        if precision not in _PRECISIONS:
+            raise ValueError(f"precision must be one of {_PRECISIONS}, got {precision!r}")
+        self.backend = backend
+        self.linear_solver = linear_solver
+        self.tol, self.max_krylov, self.max_iter = tol, max_krylov, max_iter
+        self.move, self.rho_min = move, rho_min
+        self.precision, self.levels = precision, levels
+        self.fine_degree, self.coarse_degree = fine_degree, coarse_degree
+        self.use_filter = use_filter
+        self.penal = penal
+        self.smoother = smoother
+        self.device = device
+
+    def make_state_solver(self, problem: TopologyProblem) -> StateSolver:
+        spec = problem.spec
+        if not problem.is_3d:
+            raise ValueError("SolverV4 backend currently requires a 3D problem.")
+        bc = generate_bc(spec)
+        F = problem.force_override if problem.force_override is not None else bc.F
+        outer = "fgmres" if self.linear_solver == "fgmres_gmg" else "pcg"
+        return StateSolver(problem.nel, bc.free_mask(), F, n_levels=self.levels, precision=self.precision,
+                           fine_degree=self.fine_degree, coarse_degree=self.coarse_degree, outer=outer,
+                           tol=self.tol, maxiter=self.max_krylov, smoother=self.smoother, device=self.device)
+
+    def solve(self, problem: TopologyProblem) -> OptimizationResult:
+        problem.validate()
+        loop = SIMPLoop(self, problem)
+        try:
+            history: list[dict[str, Any]] = []
+            t_total = time.perf_counter()
+            for _ in range(self.max_iter):
+                t0 = time.perf_counter()
+                row = loop.step()
+                row["wall_s"] = time.perf_counter() - t0
+                history.append(row)
+            summary = {"problem": problem.to_dict(), "backend": "SolverV4-B200",
+                       "linear_solver": "pcg_gmg" if self.linear_solver == "auto" else self.linear_solver,
+                       "precision": self.precision, "n_iter": self.max_iter,
+                       "total_wall_s": time.perf_counter() - t_total, "final": history[-1] if history else {}}
+            return OptimizationResult(problem, loop.rho.cpu().numpy(), history, summary)
+        finally:
+            loop.close()
+
+
+class SIMPLoop:
+    """One SIMP design state on the GPU, advanced by ``step()``.
+
+    A step is one SIMP iteration of the reference path (src/topogpu/solver.py:223-240):
+    state solve at the current density, then the OC update; with
+    ``use_filter`` the filtered run_simp formulation. ``step_host`` is the same
+    step with the density crossing the host boundary (pinned H2D in, D2H out).
+    """
+
+    def __init__(self, solver: SIMPSolver, problem: TopologyProblem):
+        self.solver = solver
+        self.problem = problem
+        self.state = solver.make_state_solver(problem)
+        ctx = self.state.ctx
+        dev = self.state.device
+        spec = problem.spec
+        self.volfrac = float(spec.volfrac)
+        self.rho = torch.full((ctx.n_elem,), self.volfrac, dtype=torch.float64, device=dev)
+        self.iteration = 0
+        self.rmin = None
+        if solver.use_filter:
+            self.rmin = float(problem.filter_radius or spec.rmin or 1.5)
+            self.colsum = ctx.filter(self.rmin, torch.ones_like(self.rho), transpose=True)  # H^T 1
+
+    def step(self, *, stats: bool = True) -> dict[str, Any]:
+        s, ctx = self.solver, self.state.ctx
+        if self.rmin is not None:
+            rho_phys = ctx.filter(self.rmin, self.rho)
+            compliance, dc = self.state.solve(rho_phys, s.penal)
+            dc_design = ctx.filter(self.rmin, dc, transpose=True)
+            self.rho, _ = ctx.oc_filtered(self.rho, dc_design, self.colsum, self.colsum, self.volfrac, s.move,
+                                          s.rho_min)
+        else:
+            compliance, dc = self.state.solve(self.rho, s.penal)
+            self.rho, _ = ctx.oc(self.rho, dc, self.volfrac, s.move, s.rho_min)
+        self.iteration += 1
+        row = {"iteration": self.iteration, "compliance": float(compliance),
+               "outer_iters": int(self.state.last_cg_iters), "outer_solver": self.state.last_outer_solver}
+        if stats:
+            st = ctx.field_stats(self.rho)
+            row.update({"rho_mean": st["mean"], "rho_min": st["min"], "rho_max": st["max"],
+                        "grayness": st["grayness"]})
+        return row
+
+    def step_host(self, rho_host: torch.Tensor, out_host: torch.Tensor) -> float:
+        """Upload rho (pinned host tensor), run one step, download the new rho."""
+        self.rho.copy_(rho_host, non_blocking=True)
+        row = self.step(stats=False)
+        out_host.copy_(self.rho, non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+        return row["compliance"]
+
+    def close(self):
+        self.state.close()
+
+
+def solve(problem: TopologyProblem, **kwargs: Any) -> OptimizationResult:
+    return SIMPSolver(**kwargs).solve(problem)

@@ -1,0 +1,105 @@
+"""State solve of one SIMP iteration on the device (SolverV4 equivalent).
+
+``StateSolver.solve(rho, penal) -> (compliance, dc)`` keeps the contract of
+the reference's ``SolverV4.solve`` (src/gpu_fem/solver_v4.py:147-269): E(rho),
+GMG setup, warm-started Krylov solve with a cold retry when it fails, the
+compliance F.u and the element-energy sensitivity. Everything runs in
+libtopo_b200.so; rho and dc are CUDA tensors (NumPy input is uploaded).
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from .context import TopoContext
+
+
+class StateSolver:
+    """Matrix-free GMG-preconditioned state solve on a structured hex8 grid.
+
+    Parameters mirror SolverV4's (solver_v4.py:38-89): ``n_levels``
+    (matfree_gmg_levels), ``fine_degree`` (gmg_fine_degree), ``coarse_degree``
+    (gmg_smooth_iters), ``cheb_lower`` (gmg_cheb_lower_frac), ``outer``
+    ("pcg" or "fgmres"), ``tol``/``maxiter`` (cg_tol/cg_maxiter),
+    ``warm_start``. ``precision`` selects the arithmetic schedule
+    ("fp64", "fp32" or "mixed", see include/topo_b200.h); ``smoother`` is
+    "chebyshev" (default) or "reference" (the reference V-cycle exactly).
+    """
+
+    def __init__(self, nel, free_mask, F, *, n_levels=4, precision="mixed", fine_degree=2, coarse_degree=2,
+                 cheb_lower=1.0 / 30.0, outer="pcg", restart=32, tol=1e-5, maxiter=800, warm_start=True,
+                 E0=1.0, Emin=1e-9, dense_max=16384, smoother="chebyshev", device=None):
+        if outer not in ("pcg", "fgmres"):
+            raise ValueError(f"outer must be 'pcg' or 'fgmres', got {outer!r}")
+        self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        with torch.cuda.device(self.device):
+            self.ctx = TopoContext(nel, n_levels=n_levels, mode=precision, fine_degree=fine_degree,
+                                   coarse_degree=coarse_degree, cheb_lower=cheb_lower, dense_max=dense_max,
+                                   smoother=smoother)
+        self.nel = self.ctx.nel
+        self.precision = precision
+        self.outer, self.restart = outer, restart
+        self.tol, self.maxiter = tol, maxiter
+        self.warm_start = warm_start
+        self.E0, self.Emin = E0, Emin
+        dev = self.device
+        self.free_mask = torch.as_tensor(np.asarray(free_mask, dtype=np.uint8), device=dev).contiguous()
+        self.F = torch.as_tensor(np.asarray(F, dtype=np.float64), device=dev).contiguous()
+        self.ctx.set_problem(self.free_mask, self.F)
+        self.b = (self.F * self.free_mask).contiguous()
+        self.u = torch.zeros(self.ctx.ndof, dtype=torch.float64, device=dev)
+        self.E = torch.empty(self.ctx.n_elem, dtype=torch.float64, device=dev)
+        self._have_prev = False
+        self._prev_penal = None
+        self.last_cg_iters = 0
+        self.last_relres = float("nan")
+        self.last_converged = False
+        self.last_outer_solver = outer
+        self.last_timing: dict = {}
+
+    def _krylov(self):
+        if self.outer == "pcg":
+            return self.ctx.pcg(self.b, self.u, self.tol, self.maxiter)
+        return self.ctx.fgmres(self.b, self.u, self.tol, self.maxiter, self.restart)
+
+    def solve(self, rho, penal: float = 3.0, *, timing: bool = False):
+        dev = self.device
+        rho = torch.as_tensor(rho, dtype=torch.float64, device=dev).contiguous()
+        if self._prev_penal is not None and abs(penal - self._prev_penal) > 0.5:
+            self._have_prev = False
+        self._prev_penal = penal
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)] if timing else None
+        if timing:
+            ev[0].record()
+        self.ctx.modulus(rho, penal, self.E0, self.Emin, out=self.E)
+        self.ctx.gmg_setup(self.E)
+        if timing:
+            ev[1].record()
+        warm = self.warm_start and self._have_prev
+        if not warm:
+            self.u.zero_()
+        it, rr, ok = self._krylov()
+        if not ok and warm:
+            self.u.zero_()
+            it, rr, ok = self._krylov()
+        if timing:
+            ev[2].record()
+        self.last_cg_iters, self.last_relres, self.last_converged = it, rr, ok
+        self._have_prev = True
+        compliance = self.ctx.dot(self.F, self.u)
+        dc = self.ctx.sensitivity(self.u, rho, penal, self.E0, self.Emin)
+        if timing:
+            ev[3].record()
+            torch.cuda.synchronize(dev)
+            self.last_timing = {"gmg_setup_ms": ev[0].elapsed_time(ev[1]), "cg_ms": ev[1].elapsed_time(ev[2]),
+                                "sensitivity_ms": ev[2].elapsed_time(ev[3]), "total_ms": ev[0].elapsed_time(ev[3]),
+                                "outer_solver": self.outer, "cg_iters": it}
+        return float(compliance), dc
+
+    def displacement(self) -> torch.Tensor:
+        """Last displacement (full length, fixed DoFs zero) in FP64."""
+        return self.u
+
+    def close(self):
+        self.ctx.close()
