@@ -161,6 +161,25 @@ int topo_oc_filtered(topo_ctx* ctx, const double* rho, const double* dc, const d
                      const double* colsum, double volfrac, double move, double rho_min, double* out,
                      int* out_evals, void* stream);
 
+/* Bisection OC update that allocates no device memory: the same update as
+ * topo_oc, without a context. This entry point has no counterpart in the
+ * reference. It is for callers that cannot let a library call cudaMalloc:
+ * an application whose device memory belongs to its own pool (a framework
+ * caching allocator, a Go/JVM runtime), or a latency-bound loop that cannot
+ * afford the device-wide synchronisation cudaMalloc/cudaFree may cause.
+ * rho, dc, out: n FP64 values in device memory owned by the caller.
+ * Limit: 1 <= n <= 8,388,608 elements; larger n is rejected with an error.
+ * Working memory is a 33,024-byte static device array inside the library,
+ * held by every GPU that loads it until the process exits and shared by all
+ * calls: calls that overlap on the GPU (on different streams or threads)
+ * race and must be serialised by the caller. The first call on a device
+ * looks up that array's device address (with that device current), so make
+ * it before any stream capture. Synchronises `stream` while it polls the
+ * bisection's convergence flag. out_evals (host, may be NULL) receives the
+ * number of candidate evaluations. */
+int topo_oc_noalloc(const double* rho, const double* dc, long long n, double volfrac, double move,
+                    double rho_min, double* out, int* out_evals, void* stream);
+
 /* Summary statistics of an element field (FP64): mean, min, max and
  * grayness 4 mean(x(1-x)) written to out_host[4] (synchronises the stream).
  * Replaces the history fields of src/topogpu/solver.py:120-121, 228-240. */
