@@ -151,21 +151,27 @@ def simp_steps(precision, steps, warmup, flush, rmin=2.0):
     rows = []
     for _ in range(warmup):
         rows.append(loop.step(stats=False))
-    times, launches = [], 0
+    times, launches, phases = [], 0, []
     for _ in range(steps):
         flush.zero_()
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         n0 = lib.topo_launch_count()
+        loop.state.timing = True
         e0.record()
         rows.append(loop.step(stats=False))
         e1.record()
         torch.cuda.synchronize()
         launches += int(lib.topo_launch_count() - n0)
         times.append(e0.elapsed_time(e1))
+        phases.append(dict(loop.state.last_timing))
     info = loop.state.ctx.gmg_info()
     loop.close()
-    return {"ms": times, "rows": rows, "launches": launches, "gmg": info}
+    keys = ("gmg_setup_ms", "cg_ms", "sensitivity_ms")
+    breakdown = {k: statistics.mean(ph[k] for ph in phases) for k in keys} if phases and phases[0] else {}
+    if breakdown:
+        breakdown["design_update_ms"] = statistics.mean(times) - statistics.mean(ph["total_ms"] for ph in phases)
+    return {"ms": times, "rows": rows, "launches": launches, "gmg": info, "breakdown": breakdown}
 
 
 def e2e_steps(precision, steps, warmup, flush, rmin=2.0):
@@ -285,6 +291,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp32", action="store_true")
     ap.add_argument("--micro-reps", type=int, default=100)
+    ap.add_argument("--only-ku", action="store_true", help="run only the K.u microbenchmark (profiling)")
+    ap.add_argument("--only-simp", action="store_true", help="run only the mixed SIMP steps (profiling)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
 
@@ -307,6 +315,14 @@ def main():
     lib = _lib.load()
     flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
+    if args.only_ku:
+        print(json.dumps({"ku": ku_micro(args.micro_reps)}))
+        return 0
+    if args.only_simp:
+        r = simp_steps("mixed", args.steps, args.warmup, flush)
+        print(json.dumps({"ms": r["ms"], "breakdown": r["breakdown"], "launches": r["launches"],
+                          "pcg_iters": [x["outer_iters"] for x in r["rows"]]}))
+        return 0
     micro = ku_micro(args.micro_reps)
     if dist:
         dist.barrier()
@@ -337,12 +353,12 @@ def main():
 
     pk = peaks()
     b = micro["bf16"]
-    roof = {"kernel": "k_level0<float,bf16,BF16> (level-0 K.u, BF16 input, FP32 accumulate)",
+    roof = {"kernel": "tc::k_level0_tc<float, Store> (level-0 K.u, tcgen05 BF16 input, FP32 accumulate in TMEM)",
             "workload": "192x96x48 hex8 (2,751,987 DoF), 8 rotating (u,y) pairs", "bound": "hbm",
             "achieved": b["gbs"], "peak": pk["hbm_gbs"], "unit": "GB/s", "frac": b["gbs"] / pk["hbm_gbs"],
             "traffic": None, "peak_source": pk["source"], "bytes_per_launch": b["bytes"],
             "launch_ms": b["ms"]}
-    tr = ROOT / "profiles" / "kmatvec_traffic.json"
+    tr = ROOT / "profiles" / "k_level0_tc_192x96x48_traffic.json"
     if tr.exists():
         roof["traffic"] = json.loads(tr.read_text()).get("bytes_per_launch")
 
@@ -355,10 +371,12 @@ def main():
                                  "FP32 PCG rtol 1e-5",
                        "parallelism": f"replicas x{world}", "l2": "flushed between steps (512 MB write)"},
             "pcg_iters_per_step": iters,
+            "step_breakdown_ms": mixed["breakdown"],
             "compliance_rel_err_vs_fp64": rel_err,
             "plain_fp32": None if fp32 is None else {
                 "value": world * 1e3 / (sum(fp32["ms"]) / args.steps), "ms_per_step": sum(fp32["ms"]) / args.steps,
-                "pcg_iters_per_step": [r["outer_iters"] for r in fp32["rows"][args.warmup:]]},
+                "pcg_iters_per_step": [r["outer_iters"] for r in fp32["rows"][args.warmup:]],
+                "step_breakdown_ms": fp32["breakdown"]},
             "ku": {k: {"gdof_s": v["gdof_s"], "gbs": v["gbs"], "ms": v["ms"], "gflops": v["gflops"]}
                    for k, v in micro.items()},
             "roofline": roof,

@@ -11,6 +11,7 @@
 
 #include <atomic>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <stdexcept>
@@ -148,6 +149,7 @@ struct topo_ctx {
   int cheb_form = 1;          // 0 reference recurrence, 1 Chebyshev iteration
   double lam_safety = 1.25;   // factor on the power-iteration lambda_max
   int dense_max = 16384;
+  bool use_tc = true;         // BF16 level-0 operator on tcgen05 (TOPO_B200_NO_TC=1: CUDA cores)
   std::vector<Level> L;
   Coarsest C;
   double* E64 = nullptr;
@@ -217,7 +219,8 @@ void op_apply(topo_ctx* c, int l, Prec p, const void* u, void* y, Epi epi, const
   Level& Lv = c->L[l];
   if (l == 0) {
     const void* E = (p == Prec::F64) ? (const void*)c->E64 : (const void*)c->E32;
-    level0_apply(p, Lv.g, u, E, Lv.mask, y, epi, ea, s);
+    if (p == Prec::BF16 && c->use_tc) level0_apply_tc(false, Lv.g, u, E, Lv.mask, y, epi, ea, s);
+    else level0_apply(p, Lv.g, u, E, Lv.mask, y, epi, ea, s);
   } else {
     const void* S = p == Prec::F64 ? (const void*)Lv.S64 : p == Prec::F32 ? (const void*)Lv.S32 : (const void*)Lv.S16;
     stencil_apply(p, c->vec64, Lv.g, S, u, Lv.mask, y, epi, ea, s);
@@ -591,6 +594,7 @@ int do_pcg(topo_ctx* c, const double* b, double* x, double tol, int maxiter, int
   TOPO_CUDA_CHECK(cudaMemcpyAsync(x, c->kx64, vb, cudaMemcpyDeviceToDevice, s));
   if (out_iters) *out_iters = iters;
   if (out_relres) *out_relres = bb > 0 ? std::sqrt(rr / bb) : 0.0;
+  if (c->use_tc && tc_error_flag(s)) throw std::runtime_error("tensor-core K.u: an mbarrier wait timed out");
   return converged ? 0 : 1;
 }
 
@@ -710,6 +714,9 @@ int topo_ctx_create(int nelx, int nely, int nelz, int n_levels, int mode, int fi
     std::vector<double> Q(8 * 576);
     host_galerkin_q(KE_host, Q.data());
     set_galerkin_q(Q.data());
+    tc_prepare(KE_host);
+    const char* no_tc = std::getenv("TOPO_B200_NO_TC");
+    c->use_tc = !(no_tc && no_tc[0] == '1');
     TOPO_CUDA_CHECK(cudaStreamCreateWithFlags(&c->cs, cudaStreamNonBlocking));
     TOPO_CUDA_CHECK(cudaEventCreateWithFlags(&c->ev_in, cudaEventDisableTiming));
     TOPO_CUDA_CHECK(cudaEventCreateWithFlags(&c->ev_out, cudaEventDisableTiming));
@@ -903,7 +910,10 @@ int topo_matvec(topo_ctx* c, int dtype, const void* u, void* y, const void* E, v
     EpiArgs ea{};
     if (dtype == TOPO_F64) level0_apply(Prec::F64, L0.g, u, E, L0.mask, y, Epi::Store, ea, c->cs);
     else if (dtype == TOPO_F32) level0_apply(Prec::F32, L0.g, u, E, L0.mask, y, Epi::Store, ea, c->cs);
-    else if (dtype == TOPO_BF16) level0_apply_bf16_input(L0.g, u, E, L0.mask, y, c->cs);
+    else if (dtype == TOPO_BF16) {
+      if (c->use_tc) level0_apply_tc(true, L0.g, u, E, L0.mask, y, Epi::Store, ea, c->cs);
+      else level0_apply_bf16_input(L0.g, u, E, L0.mask, y, c->cs);
+    }
     else throw std::invalid_argument("topo_matvec: bad dtype");
     return 0;
   } catch (const std::exception& e) {
@@ -941,6 +951,7 @@ int topo_gmg_apply(topo_ctx* c, const void* r, void* z, void* stream) {
     if (!c->setup_done) throw std::runtime_error("topo_gmg_apply: call topo_gmg_setup first");
     StreamGuard sg(c, stream);
     vcycle_apply(c, r, z, nullptr, c->cs);
+    if (c->use_tc && tc_error_flag(c->cs)) throw std::runtime_error("tensor-core K.u: an mbarrier wait timed out");
     return 0;
   } catch (const std::exception& e) {
     return fail(c, e);

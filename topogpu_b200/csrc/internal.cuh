@@ -209,6 +209,11 @@ __device__ __forceinline__ void epilogue_store(const EpiDev<T>& e, long long i, 
 void level0_apply(Prec p, const Grid& g, const void* u, const void* E, const uint8_t* mask, void* y,
                   Epi epi, const EpiArgs& ea, cudaStream_t s);
 void level0_diag(const Grid& g, const double* E, const uint8_t* mask, double* diag, cudaStream_t s);
+// tensor-core BF16-input operator (kmatvec_tc.cu)
+void tc_prepare(const double* KE_host);
+void level0_apply_tc(bool u_bf16, const Grid& g, const void* u, const void* E, const uint8_t* mask, void* y, Epi epi,
+                     const EpiArgs& ea, cudaStream_t s);
+int tc_error_flag(cudaStream_t s);
 void modulus(long long n, const double* rho, double penal, double E0, double Emin, double* E,
              float* E32, cudaStream_t s);
 void sensitivity(const Grid& g, const void* u, bool u_f32, const double* rho, double penal, double E0,

@@ -47,16 +47,18 @@ constexpr int NT = 128;
 constexpr uint32_t TMEM_COLS = 256;   // ZB layers x 2 parity tiles x 32 columns
 constexpr int NLEV = ZB + 1;          // output node levels staged per block
 
-// shared-memory layout (bytes, from a 1024-aligned base)
-constexpr int OFF_B = 0;                          // B operand: 32 x 32 bf16 = 2048
-constexpr int OFF_A0 = 2048;                      // node copy, even x
-constexpr int OFF_A1 = OFF_A0 + COPY_B;           // node copy, odd x
-constexpr int OFF_E = OFF_A1 + COPY_B;            // E: ZB x 16 x 16 floats
-constexpr int OFF_OUT = OFF_E + ZB * PY * PX * 4; // staged outputs
+// shared-memory layout (bytes, from a 1024-aligned base; every region 16-aligned)
+constexpr int al16(int x) { return (x + 15) & ~15; }
+constexpr int OFF_B = 0;                                 // B operand: 32 x 32 bf16 = 2048
+constexpr int OFF_A0 = 2048;                             // node copy, even x
+constexpr int OFF_A1 = OFF_A0 + COPY_B;                  // node copy, odd x
+constexpr int OFF_E = al16(OFF_A1 + COPY_B);             // E: ZB x 16 x 16 floats
+constexpr int OFF_OUT = al16(OFF_E + ZB * PY * PX * 4);  // staged outputs
 constexpr int OUT_FLOATS = OWN * OWN * NLEV * 3;
-constexpr int OFF_XCH = OFF_OUT + OUT_FLOATS * 4; // warp hand-off: 4 x 8 x 12 floats
-constexpr int OFF_BAR = OFF_XCH + 4 * 8 * 12 * 4; // ZB mbarriers
-constexpr int OFF_TMEM = OFF_BAR + ZB * 8;        // tensor-memory base address
+constexpr int OFF_XCH = al16(OFF_OUT + OUT_FLOATS * 4);  // warp hand-off: 4 x 8 x 12 floats
+constexpr int OFF_BAR = al16(OFF_XCH + 4 * 8 * 12 * 4);  // ZB mbarriers (8-byte objects)
+constexpr int OFF_TMEM = al16(OFF_BAR + ZB * 8);         // tensor-memory base address
+static_assert(OFF_BAR % 8 == 0 && OFF_TMEM % 4 == 0, "barrier alignment");
 constexpr int SMEM_BYTES = OFF_TMEM + 16 + 1024;  // + alignment slack
 // 100 KB requested so that at most two CTAs share an SM (2 x 256 TMEM columns).
 constexpr int SMEM_REQUEST = 100 * 1024;

@@ -78,7 +78,7 @@ k_level0(Grid g, const TU* __restrict__ u, const T* __restrict__ E, const uint8_
          EpiDev<T> ep, KrylovState* st, RedWork red) {
   if (st != nullptr && st->done) return;
   using TS = typename std::conditional<sizeof(T) == 8, double, float>::type;
-  __shared__ TS us[UX][UY][UZ][4];
+  __shared__ __align__(16) TS us[UX][UY][UZ][4];
   __shared__ TS es[EX][EY][EZ];
 
   const int z0 = blockIdx.x * TZ, y0 = blockIdx.y * TY, x0 = blockIdx.z * TX;
@@ -119,15 +119,51 @@ k_level0(Grid g, const TU* __restrict__ u, const T* __restrict__ E, const uint8_
 
   TS acc0 = 0, acc1 = 0, acc2 = 0;
   if (inside) {
-    TS un[3][3][3][3];
+    // Neighbour-major order: each of the 27 neighbour records is read once
+    // (one conflict-free vector load) and feeds the partial sums t[o] of
+    // every element o that contains both it and this node; then
+    // y = sum_o E_o t[o]. 576 multiply-adds, 27 shared-memory loads.
+    TS t[2][2][2][3];
+#pragma unroll
+    for (int o = 0; o < 8; ++o)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) t[o >> 2][(o >> 1) & 1][o & 1][c] = 0;
 #pragma unroll
     for (int dx = 0; dx < 3; ++dx)
 #pragma unroll
       for (int dy = 0; dy < 3; ++dy)
 #pragma unroll
-        for (int dz = 0; dz < 3; ++dz)
+        for (int dz = 0; dz < 3; ++dz) {
+          const TS* rec = &us[tx + dx][ty + dy][tz + dz][0];
+          TS uv[3];
+          if constexpr (sizeof(TS) == 4) {
+            const float4 v = *reinterpret_cast<const float4*>(rec);
+            uv[0] = v.x;
+            uv[1] = v.y;
+            uv[2] = v.z;
+          } else {
+            const double2 v01 = *reinterpret_cast<const double2*>(rec);
+            uv[0] = v01.x;
+            uv[1] = v01.y;
+            uv[2] = rec[2];
+          }
 #pragma unroll
-          for (int c = 0; c < 3; ++c) un[dx][dy][dz][c] = us[tx + dx][ty + dy][tz + dz][c];
+          for (int ox = 0; ox < 2; ++ox)
+#pragma unroll
+            for (int oy = 0; oy < 2; ++oy)
+#pragma unroll
+              for (int oz = 0; oz < 2; ++oz) {
+                const int mx = dx - ox, my = dy - oy, mz = dz - oz;  // neighbour's corner in element o
+                if (mx < 0 || mx > 1 || my < 0 || my > 1 || mz < 0 || mz > 1) continue;
+                const int a = corner_id(1 - ox, 1 - oy, 1 - oz);
+                const int m = corner_id(mx, my, mz);
+#pragma unroll
+                for (int c = 0; c < 3; ++c)
+#pragma unroll
+                  for (int d = 0; d < 3; ++d)
+                    t[ox][oy][oz][c] += ke<TS, BF>((3 * a + c) * 24 + 3 * m + d) * uv[d];
+              }
+        }
 #pragma unroll
     for (int ox = 0; ox < 2; ++ox)
 #pragma unroll
@@ -135,26 +171,9 @@ k_level0(Grid g, const TU* __restrict__ u, const T* __restrict__ E, const uint8_
 #pragma unroll
         for (int oz = 0; oz < 2; ++oz) {
           const TS Ee = es[tx + ox][ty + oy][tz + oz];
-          const int a = corner_id(1 - ox, 1 - oy, 1 - oz);
-          TS t0 = 0, t1 = 0, t2 = 0;
-#pragma unroll
-          for (int mx = 0; mx < 2; ++mx)
-#pragma unroll
-            for (int my = 0; my < 2; ++my)
-#pragma unroll
-              for (int mz = 0; mz < 2; ++mz) {
-                const int m = corner_id(mx, my, mz);
-#pragma unroll
-                for (int d = 0; d < 3; ++d) {
-                  const TS uv = un[ox + mx][oy + my][oz + mz][d];
-                  t0 += ke<TS, BF>((3 * a + 0) * 24 + 3 * m + d) * uv;
-                  t1 += ke<TS, BF>((3 * a + 1) * 24 + 3 * m + d) * uv;
-                  t2 += ke<TS, BF>((3 * a + 2) * 24 + 3 * m + d) * uv;
-                }
-              }
-          acc0 += Ee * t0;
-          acc1 += Ee * t1;
-          acc2 += Ee * t2;
+          acc0 += Ee * t[ox][oy][oz][0];
+          acc1 += Ee * t[ox][oy][oz][1];
+          acc2 += Ee * t[ox][oy][oz][2];
         }
   }
 

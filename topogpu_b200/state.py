@@ -63,8 +63,11 @@ class StateSolver:
             return self.ctx.pcg(self.b, self.u, self.tol, self.maxiter)
         return self.ctx.fgmres(self.b, self.u, self.tol, self.maxiter, self.restart)
 
+    timing = False  # set True to fill last_timing on every solve (adds one sync)
+
     def solve(self, rho, penal: float = 3.0, *, timing: bool = False):
         dev = self.device
+        timing = timing or self.timing
         rho = torch.as_tensor(rho, dtype=torch.float64, device=dev).contiguous()
         if self._prev_penal is not None and abs(penal - self._prev_penal) > 0.5:
             self._have_prev = False
