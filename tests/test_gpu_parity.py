@@ -214,7 +214,11 @@ def test_pcg_and_fgmres_fp64_match_reference(cuda_dev, tag, nel, nlev):
     b = _t(bc.F)
     x = torch.zeros_like(b)
     it, rr, ok = ctx.pcg(b, x, tol=1e-8, maxiter=500)
-    assert ok and it == int(g[f"pcg_it_{tag}"]) and rr < 1e-8
+    # On 7x5x3 the reference's relative residual after 45 iterations is
+    # 1.077e-8, 8% above the tolerance: a 1e-16 relative perturbation of K.u
+    # in the oracle already moves the stop between 45 and 46 (FGMRES stays at
+    # its count), so PCG is held to +-1 iteration and the solution to 1e-9.
+    assert ok and abs(it - int(g[f"pcg_it_{tag}"])) <= 1 and rr < 1e-8
     assert _rel(x.cpu().numpy()[bc.free], g[f"pcg_x_{tag}"]) < 1e-9
     x2 = torch.zeros_like(b)
     it2, rr2, ok2 = ctx.fgmres(b, x2, tol=1e-8, maxiter=500, restart=32)

@@ -461,30 +461,35 @@ void dense_assemble(const Grid& g, const double* S, const int* dof_index, int n,
 
 // Banded right-looking Cholesky on dense row-major storage, panel width CNB.
 // The band half-width `band` bounds every non-zero (|i-j| <= band), and the
-// factor keeps the same band, so only that window is touched.
+// factor keeps the same band, so only that window is touched. The factored
+// diagonal blocks go to a side array Dt (one CNB x CNB lower block per panel,
+// identity-padded past n); the off-diagonal band of L overwrites A's lower
+// part. A's diagonal blocks keep their updated, unfactored values and are not
+// read as L afterwards.
 constexpr int CNB = 32;
 
-// Factor the CNB x CNB diagonal block at (k,k) in shared memory.
-__global__ void k_chol_diag(int n, int k, double* __restrict__ A, int* __restrict__ flag) {
+// One panel step. Every CTA factors the (k,k) block in shared memory (the
+// same arithmetic in each, so all agree); CTA 0 stores it in Dt and raises
+// `flag` on a non-positive or non-finite pivot (the pivot is then taken as
+// 1). Each thread then solves one panel row i in [k+nb, min(n, k+nb+band)):
+// L_ik L_kk^T = A_ik.
+__global__ void k_chol_step(int n, int k, int band, double* __restrict__ A, double* __restrict__ Dt,
+                            int* __restrict__ flag) {
   __shared__ double L[CNB][CNB + 1];
   const int nb = min(CNB, n - k);
-  for (int q = threadIdx.x; q < nb * nb; q += blockDim.x) {
-    const int i = q / nb, j = q % nb;
-    L[i][j] = A[(long long)(k + i) * n + k + j];
+  for (int q = threadIdx.x; q < CNB * CNB; q += blockDim.x) {
+    const int i = q / CNB, j = q % CNB;
+    L[i][j] = (i < nb && j < nb) ? A[(long long)(k + i) * n + k + j] : (i == j ? 1.0 : 0.0);
   }
   __syncthreads();
+  bool bad = false;
   for (int j = 0; j < nb; ++j) {
-    if (threadIdx.x == 0) {
-      const double d = L[j][j];
-      if (!(d > 0.0) || !isfinite(d)) {
-        *flag = 1;
-        L[j][j] = 1.0;
-      } else {
-        L[j][j] = sqrt(d);
-      }
-    }
+    const double d = L[j][j];
+    const bool ok = d > 0.0 && isfinite(d);
+    bad |= !ok;
+    const double ljj = ok ? sqrt(d) : 1.0;
     __syncthreads();
-    const double ljj = L[j][j];
+    if (threadIdx.x == 0) L[j][j] = ljj;
     for (int i = j + 1 + threadIdx.x; i < nb; i += blockDim.x) L[i][j] /= ljj;
     __syncthreads();
     for (int q = threadIdx.x; q < (nb - j - 1) * (nb - j - 1); q += blockDim.x) {
@@ -493,18 +498,14 @@ __global__ void k_chol_diag(int n, int k, double* __restrict__ A, int* __restric
     }
     __syncthreads();
   }
-  for (int q = threadIdx.x; q < nb * nb; q += blockDim.x) {
-    const int i = q / nb, j = q % nb;
-    A[(long long)(k + i) * n + k + j] = (j <= i) ? L[i][j] : 0.0;
+  if (blockIdx.x == 0) {
+    double* D = Dt + (long long)(k / CNB) * CNB * CNB;
+    for (int q = threadIdx.x; q < CNB * CNB; q += blockDim.x) {
+      const int i = q / CNB, j = q % CNB;
+      D[q] = (j <= i) ? L[i][j] : 0.0;
+    }
+    if (threadIdx.x == 0 && bad) *flag = 1;
   }
-}
-
-// Panel: rows i in [k+nb, min(n, k+nb+band)) solve L_ik L_kk^T = A_ik.
-__global__ void k_chol_panel(int n, int k, int band, double* __restrict__ A) {
-  __shared__ double L[CNB][CNB + 1];
-  const int nb = min(CNB, n - k);
-  for (int q = threadIdx.x; q < nb * nb; q += blockDim.x) L[q / nb][q % nb] = A[(long long)(k + q / nb) * n + k + q % nb];
-  __syncthreads();
   const int i = k + nb + blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n || i >= k + nb + band) return;
   double x[CNB];
@@ -548,66 +549,131 @@ __global__ void k_chol_update(int n, int k, int band, double* __restrict__ A) {
   A[(long long)i * n + j] -= s;
 }
 
-// U = L^T (row-major): U[i][t] = L[t][i] for t in [i, i+band].
-__global__ void k_transpose_band(int n, int band, const double* __restrict__ L, double* __restrict__ U) {
-  const int i = blockIdx.x;
-  for (int t = i + threadIdx.x; t < n && t <= i + band; t += blockDim.x) U[(long long)i * n + t] = L[(long long)t * n + i];
-}
-
-// Column j of K^-1 from the banded factor: forward y = L^-1 e_j (rows >= j),
-// then backward x = L^-T y down to row j; x[i] for i >= j is written to
-// column-major lower storage Xc[j*n + i]. One warp per column.
-__global__ void k_inverse_columns(int n, int band, const double* __restrict__ L, const double* __restrict__ U,
-                                  double* __restrict__ Xc) {
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (warp >= n) return;
-  const int j = warp;
-  double* y = Xc + (long long)j * n;  // working column (rows j..n-1)
-  for (int i = j; i < n; ++i) {
-    const double* Li = L + (long long)i * n;
-    const int t0 = max(j, i - band);
-    double s = 0.0;
-    for (int t = t0 + lane; t < i; t += 32) s += Li[t] * y[t];
-    s = warp_sum(s);
-    if (lane == 0) y[i] = ((i == j ? 1.0 : 0.0) - s) / Li[i];
-    __syncwarp();
+// Inverse of every factored diagonal block (identity-padded, so the last
+// partial block inverts cleanly): thread j forms column j by forward
+// substitution.
+__global__ void k_block_tri_inv(const double* __restrict__ Dt, double* __restrict__ Di) {
+  __shared__ double L[CNB][CNB + 1];
+  __shared__ double X[CNB][CNB + 1];
+  const long long base = (long long)blockIdx.x * CNB * CNB;
+  for (int q = threadIdx.x; q < CNB * CNB; q += blockDim.x) L[q / CNB][q % CNB] = Dt[base + q];
+  __syncthreads();
+  const int j = threadIdx.x;
+  for (int i = 0; i < CNB; ++i) {
+    double v = (i == j) ? 1.0 : 0.0;
+    for (int m = j; m < i; ++m) v -= L[i][m] * X[m][j];
+    X[i][j] = v / L[i][i];
   }
-  for (int i = n - 1; i >= j; --i) {
-    const double* Ui = U + (long long)i * n;
-    const int t1 = min(n - 1, i + band);
-    double s = 0.0;
-    for (int t = i + 1 + lane; t <= t1; t += 32) s += Ui[t] * y[t];
-    s = warp_sum(s);
-    if (lane == 0) y[i] = (y[i] - s) / Ui[i];
-    __syncwarp();
+  __syncthreads();
+  for (int q = threadIdx.x; q < CNB * CNB; q += blockDim.x) Di[base + q] = X[q / CNB][q % CNB];
+}
+
+// W = L^-1 by block forward substitution in CNB-row steps. CTA J owns the
+// column block J; for I = J .. nT-1
+//   R    = delta_IJ Id - sum_{k in [max(32J, 32I-band), 32I)} L[32I.., k] W[k, 32J..]
+//   W_IJ = Di_I R
+// Every W read is of rows this CTA wrote in an earlier step (visible after
+// __syncthreads), so the column blocks run independently with no grid sync.
+// W goes to W64 (lower part, FP64) and to the apply matrices C64 / C32 as W
+// in the lower triangle and W^T in the strict upper triangle. All three
+// share the row stride ldc. The K-loop stages 32-wide chunks of L and W in
+// shared memory with the next chunk prefetched into registers.
+constexpr int TIT = 256;
+__global__ void __launch_bounds__(TIT) k_tri_inverse(int n, int band, const double* __restrict__ L,
+                                                     const double* __restrict__ Di, double* W64, long long ldc,
+                                                     double* C64, float* C32) {
+  __shared__ double Ls[CNB][CNB + 1];
+  __shared__ __align__(16) double Ws[CNB][CNB + 2];
+  __shared__ double Rs[CNB][CNB + 1];
+  __shared__ double Ds[CNB][CNB + 1];
+  const int J = blockIdx.x, nT = gridDim.x;
+  const int t = threadIdx.x, r = t >> 3, cq = (t & 7) * 4;
+  const int j0 = J * CNB;
+  double pl[4], pw[4];
+  for (int I = J; I < nT; ++I) {
+    const int i0 = I * CNB;
+    const int klo = max(j0, i0 - band);
+    auto fetch = [&](int k0) {
+#pragma unroll
+      for (int m = 0; m < 4; ++m) {
+        const int q = t + TIT * m, hi = q >> 5, lo = q & 31;
+        const int i = i0 + hi, k = k0 + lo;
+        pl[m] = (i < n && k < i0) ? L[(long long)i * n + k] : 0.0;
+        const int kw = k0 + hi, cw = j0 + lo;
+        pw[m] = (kw < i0 && cw < n && cw <= kw) ? W64[(long long)kw * ldc + cw] : 0.0;
+      }
+    };
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    if (klo < i0) fetch(klo);
+    for (int k0 = klo; k0 < i0; k0 += CNB) {
+      __syncthreads();
+#pragma unroll
+      for (int m = 0; m < 4; ++m) {
+        const int q = t + TIT * m;
+        Ls[q >> 5][q & 31] = pl[m];
+        Ws[q >> 5][q & 31] = pw[m];
+      }
+      __syncthreads();
+      if (k0 + CNB < i0) fetch(k0 + CNB);
+#pragma unroll 8
+      for (int kk = 0; kk < CNB; ++kk) {
+        const double a = Ls[r][kk];
+        const double2 w01 = *reinterpret_cast<const double2*>(&Ws[kk][cq]);
+        const double2 w23 = *reinterpret_cast<const double2*>(&Ws[kk][cq + 2]);
+        acc[0] = fma(a, w01.x, acc[0]);
+        acc[1] = fma(a, w01.y, acc[1]);
+        acc[2] = fma(a, w23.x, acc[2]);
+        acc[3] = fma(a, w23.y, acc[3]);
+      }
+    }
+    for (int q = t; q < CNB * CNB; q += TIT) Ds[q >> 5][q & 31] = Di[(long long)I * CNB * CNB + q];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) Rs[r][cq + q] = ((i0 + r == j0 + cq + q) ? 1.0 : 0.0) - acc[q];
+    __syncthreads();
+    double w[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int m = 0; m <= r; ++m) {
+      const double d = Ds[r][m];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) w[q] = fma(d, Rs[m][cq + q], w[q]);
+    }
+    __syncthreads();
+    const int i = i0 + r;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int c = j0 + cq + q;
+      Rs[r][cq + q] = w[q];
+      if (i < n && c < n && c <= i) {
+        W64[(long long)i * ldc + c] = w[q];
+        if (C64 != nullptr && C64 != W64) C64[(long long)i * ldc + c] = w[q];
+        if (C32 != nullptr) C32[(long long)i * ldc + c] = (float)w[q];
+      }
+    }
+    __syncthreads();
+    // transposed copy: thread -> row j0 + (t >> 3), columns i0 + (t & 7) * 4 + q
+    if (C64 != nullptr || C32 != nullptr) {
+      const int cr = j0 + r;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int ic = i0 + cq + q;
+        if (cr < n && ic < n && ic > cr) {
+          const double v = Rs[cq + q][r];
+          if (C64 != nullptr) C64[(long long)cr * ldc + ic] = v;
+          if (C32 != nullptr) C32[(long long)cr * ldc + ic] = (float)v;
+        }
+      }
+    }
+    __syncthreads();
   }
 }
 
-// Full row-major inverse (FP64 and FP32 copies) from the lower column store.
-__global__ void k_mirror(int n, const double* __restrict__ Xc, double* __restrict__ X64, float* __restrict__ X32) {
-  const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (q >= (long long)n * n) return;
-  const int i = (int)(q / n), j = (int)(q % n);
-  const double v = (i >= j) ? Xc[(long long)j * n + i] : Xc[(long long)i * n + j];
-  if (X64) X64[q] = v;
-  if (X32) X32[q] = (float)v;
-}
-
-int dense_cholesky_inverse(int n, int band, double* A, double* Ainv, double* work, int* flag, cudaStream_t s) {
-  // A (n*n): assembled matrix, factorised in place into L.
-  // work (n*n): U = L^T, then reused as the column-major inverse store.
-  // Ainv: receives nothing here; the caller mirrors with dense_mirror.
-  (void)Ainv;
+int dense_cholesky(int n, int band, double* A, double* Dt, int* flag, cudaStream_t s) {
   TOPO_CUDA_CHECK(cudaMemsetAsync(flag, 0, sizeof(int), s));
   for (int k = 0; k < n; k += CNB) {
     const int nb = std::min(CNB, n - k);
-    k_chol_diag<<<1, 256, 0, s>>>(n, k, A, flag);
-    TOPO_LAUNCH_CHECK();
     const int rows = std::min(n - (k + nb), band);
+    k_chol_step<<<std::max(1, (rows + 127) / 128), 128, 0, s>>>(n, k, band, A, Dt, flag);
+    TOPO_LAUNCH_CHECK();
     if (rows > 0) {
-      k_chol_panel<<<(rows + 127) / 128, 128, 0, s>>>(n, k, band, A);
-      TOPO_LAUNCH_CHECK();
       dim3 blk(16, 16), grd((rows + 15) / 16, (rows + 15) / 16);
       k_chol_update<<<grd, blk, 0, s>>>(n, k, band, A);
       TOPO_LAUNCH_CHECK();
@@ -616,64 +682,97 @@ int dense_cholesky_inverse(int n, int band, double* A, double* Ainv, double* wor
   int h_flag = 0;
   TOPO_CUDA_CHECK(cudaMemcpyAsync(&h_flag, flag, sizeof(int), cudaMemcpyDeviceToHost, s));
   TOPO_CUDA_CHECK(cudaStreamSynchronize(s));
-  if (h_flag) return 1;
-  // U = L^T into work, then inverse columns into A's storage? A holds L and is
-  // still needed; use Ainv as the column store.
-  k_transpose_band<<<n, 128, 0, s>>>(n, band, A, work);
-  TOPO_LAUNCH_CHECK();
-  const int warps_per_block = 4;
-  k_inverse_columns<<<(n + warps_per_block - 1) / warps_per_block, 32 * warps_per_block, 0, s>>>(n, band, A, work,
-                                                                                                Ainv);
-  TOPO_LAUNCH_CHECK();
-  return 0;
+  return h_flag ? 1 : 0;
 }
 
-void dense_mirror(int n, const double* Xc, double* X64, float* X32, cudaStream_t s) {
-  const long long nn = (long long)n * n;
-  k_mirror<<<(unsigned)((nn + 255) / 256), 256, 0, s>>>(n, Xc, X64, X32);
+void dense_inverse_factor(int n, int band, const double* A, const double* Dt, double* Di, double* W64, long long ldc,
+                          double* C64, float* C32, cudaStream_t s) {
+  const int nT = (n + CNB - 1) / CNB;
+  k_block_tri_inv<<<nT, CNB, 0, s>>>(Dt, Di);
+  TOPO_LAUNCH_CHECK();
+  k_tri_inverse<<<nT, TIT, 0, s>>>(n, band, A, Di, W64, ldc, C64, C32);
   TOPO_LAUNCH_CHECK();
 }
 
-// x = mask-scatter(X * gather(r)): one warp per row of the full inverse.
+// Coarsest solve z = W^T (W r) = K^-1 r with W = L^-1, in two passes over the
+// combined matrix C (W below and on the diagonal, W^T above): pass one
+// y = W r_c (row i reads C[i][0..i]), pass two z_c = W^T y (row j reads
+// C[j][j..n-1]). One warp per row, 16-byte loads (rows are padded to ldc, a
+// multiple of 32 elements, so every row starts 16-byte aligned), FP64
+// accumulation, the compact vector staged in shared memory.
 template <typename T, typename TX>
-__global__ void k_dense_gemv(int n, const TX* __restrict__ X, const int* __restrict__ free_list,
-                             const T* __restrict__ rhs, T* __restrict__ x, const KrylovState* st) {
+__global__ void k_coarse_lower(int n, long long ldc, const TX* __restrict__ C, const int* __restrict__ free_list,
+                               const T* __restrict__ rhs, double* __restrict__ y, const KrylovState* st) {
   if (st != nullptr && st->done) return;
-  extern __shared__ unsigned char smem_raw[];
-  T* rc = reinterpret_cast<T*>(smem_raw);
-  for (int j = threadIdx.x; j < n; j += blockDim.x) rc[j] = rhs[free_list[j]];
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double* rc = reinterpret_cast<double*>(smem_raw);
+  for (int j = threadIdx.x; j < n; j += blockDim.x) rc[j] = (double)rhs[free_list[j]];
   __syncthreads();
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (warp >= n) return;
-  const TX* row = X + (long long)warp * n;
+  const int row = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+  if (row >= n) return;
+  constexpr int V = 16 / sizeof(TX);
+  const TX* Ci = C + (long long)row * ldc;
   double acc = 0.0;
-  for (int j = lane; j < n; j += 32) acc += (double)row[j] * (double)rc[j];
+  for (int j = lane * V; j <= row; j += 32 * V) {
+    TX v[V];
+    *reinterpret_cast<uint4*>(v) = *reinterpret_cast<const uint4*>(Ci + j);
+#pragma unroll
+    for (int q = 0; q < V; ++q)
+      if (j + q <= row) acc += (double)v[q] * rc[j + q];
+  }
   acc = warp_sum(acc);
-  if (lane == 0) x[free_list[warp]] = (T)acc;
+  if (lane == 0) y[row] = acc;
 }
 
-// The compact right-hand side is staged in shared memory: opt in to more than
-// 48 KB when the coarsest system is large (B200 allows up to 227 KB per block).
-void dense_gemv_prepare(int n) {
-  const int b64 = (int)(sizeof(double) * n), b32 = (int)(sizeof(float) * n);
-  if (b64 > 227 * 1024) throw std::runtime_error("coarsest system too large for the shared-memory GEMV");
-  TOPO_CUDA_CHECK(cudaFuncSetAttribute(k_dense_gemv<double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       std::max(b64, 48 * 1024)));
-  TOPO_CUDA_CHECK(cudaFuncSetAttribute(k_dense_gemv<float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       std::max(b32, 48 * 1024)));
+template <typename T, typename TX>
+__global__ void k_coarse_upper(int n, long long ldc, const TX* __restrict__ C, const int* __restrict__ free_list,
+                               const double* __restrict__ y, T* __restrict__ x, const KrylovState* st) {
+  if (st != nullptr && st->done) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double* ys = reinterpret_cast<double*>(smem_raw);
+  for (int j = threadIdx.x; j < n; j += blockDim.x) ys[j] = y[j];
+  __syncthreads();
+  const int row = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+  if (row >= n) return;
+  constexpr int V = 16 / sizeof(TX);
+  const TX* Cj = C + (long long)row * ldc;
+  double acc = 0.0;
+  for (int i = (row / V) * V + lane * V; i < n; i += 32 * V) {
+    TX v[V];
+    *reinterpret_cast<uint4*>(v) = *reinterpret_cast<const uint4*>(Cj + i);
+#pragma unroll
+    for (int q = 0; q < V; ++q)
+      if (i + q >= row && i + q < n) acc += (double)v[q] * ys[i + q];
+  }
+  acc = warp_sum(acc);
+  if (lane == 0) x[free_list[row]] = (T)acc;
 }
 
-void dense_gemv(bool vec64, int n, const double* A64, const float* A32, const int* free_list, const void* rhs,
-                void* x, const KrylovState* st, cudaStream_t s) {
+// The compact vectors are staged in shared memory: opt in to more than 48 KB
+// when the coarsest system is large (B200 allows up to 227 KB per block).
+void dense_apply_prepare(int n) {
+  const int b = (int)(sizeof(double) * n);
+  if (b > 227 * 1024) throw std::runtime_error("coarsest system too large for the shared-memory solve");
+  const int a = std::max(b, 48 * 1024);
+  TOPO_CUDA_CHECK(cudaFuncSetAttribute(k_coarse_lower<double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, a));
+  TOPO_CUDA_CHECK(cudaFuncSetAttribute(k_coarse_lower<float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, a));
+  TOPO_CUDA_CHECK(cudaFuncSetAttribute(k_coarse_upper<double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, a));
+  TOPO_CUDA_CHECK(cudaFuncSetAttribute(k_coarse_upper<float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, a));
+}
+
+void dense_apply(bool vec64, int n, long long ldc, const double* C64, const float* C32, const int* free_list,
+                 const void* rhs, double* y, void* x, const KrylovState* st, cudaStream_t s) {
   const int wpb = 8;
   const unsigned nb = (unsigned)((n + wpb - 1) / wpb);
+  const size_t sh = sizeof(double) * n;
   if (vec64) {
-    const size_t sh = sizeof(double) * n;
-    k_dense_gemv<double, double><<<nb, 32 * wpb, sh, s>>>(n, A64, free_list, (const double*)rhs, (double*)x, st);
+    k_coarse_lower<double, double><<<nb, 32 * wpb, sh, s>>>(n, ldc, C64, free_list, (const double*)rhs, y, st);
+    TOPO_LAUNCH_CHECK();
+    k_coarse_upper<double, double><<<nb, 32 * wpb, sh, s>>>(n, ldc, C64, free_list, y, (double*)x, st);
   } else {
-    const size_t sh = sizeof(float) * n;
-    k_dense_gemv<float, float><<<nb, 32 * wpb, sh, s>>>(n, A32, free_list, (const float*)rhs, (float*)x, st);
+    k_coarse_lower<float, float><<<nb, 32 * wpb, sh, s>>>(n, ldc, C32, free_list, (const float*)rhs, y, st);
+    TOPO_LAUNCH_CHECK();
+    k_coarse_upper<float, float><<<nb, 32 * wpb, sh, s>>>(n, ldc, C32, free_list, y, (float*)x, st);
   }
   TOPO_LAUNCH_CHECK();
 }

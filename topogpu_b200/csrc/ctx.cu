@@ -22,8 +22,6 @@ namespace topo {
 
 void level0_apply_bf16_input(const Grid& g, const void* u, const void* E, const uint8_t* mask, void* y,
                              cudaStream_t s);
-void dense_mirror(int n, const double* Xc, double* X64, float* X32, cudaStream_t s);
-void dense_gemv_prepare(int n);
 
 static std::atomic<long long> g_launches{0};
 void count_launches(long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
@@ -124,10 +122,13 @@ struct Coarsest {
   int kind = 0;  // 0 none, 1 dense, 2 regularised dense
   int* dof_index = nullptr;
   int* free_list = nullptr;
-  double* A = nullptr;
-  double* work = nullptr;
-  double* Xc = nullptr;
-  float* X32 = nullptr;
+  long long ldc = 0;        // row stride of work / X32 (n rounded up to 32)
+  double* A = nullptr;      // assembled matrix, then the band of L
+  double* Dt = nullptr;     // factored diagonal blocks of L (32x32 each)
+  double* Di = nullptr;     // their inverses
+  double* work = nullptr;   // W = L^-1 (FP64); with FP64 vectors also W^T above the diagonal
+  float* X32 = nullptr;     // FP32 W / W^T apply matrix (FP32 vectors)
+  double* y = nullptr;      // compact FP64 intermediate of the two-pass apply
   int* flag = nullptr;
   double* tmp = nullptr;   // FP64 Jacobi inverse of a coarse level when vectors are FP32
   double* scrA = nullptr;  // FP64 scratch vectors for the coarse power iterations
@@ -276,7 +277,7 @@ void coarsest_solve(topo_ctx* c, const KrylovState* st, cudaStream_t s) {
   else k_gather_zero<float><<<gblocks(n_full), 256, 0, s>>>(n_full, (float*)Lv.x);
   TOPO_LAUNCH_CHECK();
   if (c->C.n == 0) return;
-  dense_gemv(c->vec64, c->C.n, c->C.work, c->C.X32, c->C.free_list, Lv.b, Lv.x, st, s);
+  dense_apply(c->vec64, c->C.n, c->C.ldc, c->C.work, c->C.X32, c->C.free_list, Lv.b, c->C.y, Lv.x, st, s);
 }
 
 // One V-cycle on level l (multigrid_v4.py:986-1008): input Lv.b, output Lv.x.
@@ -457,7 +458,7 @@ void do_setup(topo_ctx* c, const double* E, cudaStream_t s) {
     Level& Lc = c->L[l];
     const int n = c->C.n;
     dense_assemble(Lc.g, Lc.S64, c->C.dof_index, n, c->C.A, s);
-    int bad = dense_cholesky_inverse(n, c->C.band, c->C.A, c->C.Xc, c->C.work, c->C.flag, s);
+    int bad = dense_cholesky(n, c->C.band, c->C.A, c->C.Dt, c->C.flag, s);
     if (bad) {
       dense_assemble(Lc.g, Lc.S64, c->C.dof_index, n, c->C.A, s);
       k_diag_sum<<<1, 256, 0, s>>>(n, c->C.A, c->dtmp);
@@ -468,13 +469,14 @@ void do_setup(topo_ctx* c, const double* E, cudaStream_t s) {
       const double eps = std::max(dsum / n * 1e-8, 1e-14);
       k_add_diag<<<(n + 255) / 256, 256, 0, s>>>(n, c->C.A, eps);
       TOPO_LAUNCH_CHECK();
-      bad = dense_cholesky_inverse(n, c->C.band, c->C.A, c->C.Xc, c->C.work, c->C.flag, s);
+      bad = dense_cholesky(n, c->C.band, c->C.A, c->C.Dt, c->C.flag, s);
       if (bad) throw std::runtime_error("coarsest-level Cholesky failed even after eps*I regularisation");
       c->C.kind = 2;
     } else {
       c->C.kind = 1;
     }
-    dense_mirror(n, c->C.Xc, c->C.work, c->vec64 ? nullptr : c->C.X32, s);
+    dense_inverse_factor(n, c->C.band, c->C.A, c->C.Dt, c->C.Di, c->C.work, c->C.ldc,
+                         c->vec64 ? c->C.work : nullptr, c->vec64 ? nullptr : c->C.X32, s);
   }
   TOPO_CUDA_CHECK(cudaStreamSynchronize(s));
   c->setup_done = true;
@@ -870,11 +872,15 @@ int topo_set_problem(topo_ctx* c, const uint8_t* free_mask, const double* F, voi
         c->C.n = n;
         c->C.dof_index = c->alloc<int>(Lc.g.ndof);
         c->C.free_list = c->alloc<int>(std::max(n, 1));
+        const long long nt = (n + 31) / 32;
+        c->C.ldc = nt * 32;
         c->C.A = c->alloc<double>((long long)n * n);
-        c->C.work = c->alloc<double>((long long)n * n);
-        c->C.Xc = c->alloc<double>((long long)n * n);
-        if (!c->vec64) c->C.X32 = c->alloc<float>((long long)n * n);
-        dense_gemv_prepare(n);
+        c->C.Dt = c->alloc<double>(nt * 1024);
+        c->C.Di = c->alloc<double>(nt * 1024);
+        c->C.work = c->alloc<double>((long long)n * c->C.ldc);
+        if (!c->vec64) c->C.X32 = c->alloc<float>((long long)n * c->C.ldc);
+        c->C.y = c->alloc<double>(std::max(n, 1));
+        dense_apply_prepare(n);
       }
       c->C.band = band;
       TOPO_CUDA_CHECK(cudaMemcpyAsync(c->C.dof_index, idx.data(), sizeof(int) * idx.size(), cudaMemcpyHostToDevice, s));

@@ -237,11 +237,18 @@ void prolong_add(bool vec64, const Grid& fine, const Grid& coarse, const void* e
                  void* xf, void* e_out, const KrylovState* st, cudaStream_t s);
 void dense_assemble(const Grid& g, const double* S, const int* dof_index, int n, double* A,
                     cudaStream_t s);
-// returns 0 on success, 1 if a pivot was not positive/finite (host sync inside)
-int dense_cholesky_inverse(int n, int band, double* A, double* Ainv, double* work, int* flag,
-                           cudaStream_t s);
-void dense_gemv(bool vec64, int n, const double* A64, const float* A32, const int* dof_index,
-                const void* rhs, void* x, const KrylovState* st, cudaStream_t s);
+// Banded Cholesky in place (off-diagonal band of L in A's lower part, the
+// factored diagonal blocks in Dt); returns 0 on success, 1 if a pivot was not
+// positive/finite (host sync inside).
+int dense_cholesky(int n, int band, double* A, double* Dt, int* flag, cudaStream_t s);
+// W = L^-1 into W64 (FP64, lower) and into the apply matrices C64/C32 (W
+// lower, W^T upper); Di receives the inverses of the diagonal blocks.
+void dense_inverse_factor(int n, int band, const double* A, const double* Dt, double* Di, double* W64,
+                          long long ldc, double* C64, float* C32, cudaStream_t s);
+void dense_apply_prepare(int n);
+// x = scatter(W^T W gather(rhs)); y is n FP64 scratch
+void dense_apply(bool vec64, int n, long long ldc, const double* C64, const float* C32, const int* free_list,
+                 const void* rhs, double* y, void* x, const KrylovState* st, cudaStream_t s);
 
 // vectors and reductions (vec.cu)
 void vfill(bool f64, long long n, void* x, double v, cudaStream_t s);
