@@ -166,6 +166,7 @@ def simp_steps(precision, steps, warmup, flush, rmin=2.0):
         times.append(e0.elapsed_time(e1))
         phases.append(dict(loop.state.last_timing))
     info = loop.state.ctx.gmg_info()
+    info["setup_phases_ms"] = loop.state.ctx.setup_phases()
     loop.close()
     keys = ("gmg_setup_ms", "cg_ms", "sensitivity_ms")
     breakdown = {k: statistics.mean(ph[k] for ph in phases) for k in keys} if phases and phases[0] else {}

@@ -189,6 +189,13 @@ int topo_field_stats(topo_ctx* ctx, const double* x, long long n, double* out_ho
  * coarsest solve kind (0 none, 1 dense Cholesky, 2 regularised Cholesky,
  * 3 iterative). Arrays have n_levels entries. */
 int topo_gmg_info(topo_ctx* ctx, long long* n_free, double* lambda_max, int* coarse_kind);
+/* Device time (ms) of the phases of the last topo_gmg_setup: ms[0] fine
+ * diagonal and lambda_max check, ms[1] coarse stencils (level-1 Galerkin,
+ * R.A.P, Jacobi, lambda, conversions), ms[2] coarsest dense assembly,
+ * ms[3] banded Cholesky, ms[4] W = L^-1. Diagnostic of GalerkinMatFreeGMG.setup
+ * (src/gpu_fem/multigrid_v4.py:657-811), which the reference times only as a
+ * whole in SolverV4.last_timing (solver_v4.py:231-267). */
+int topo_setup_phases(topo_ctx* ctx, double* ms);
 
 /* Copy the FP64 operator of coarse level `level` (1..n_levels-1) from the
  * last setup into S_out (device, 243*nnodes_level doubles): the 3x3 block

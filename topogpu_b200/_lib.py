@@ -44,6 +44,7 @@ SIGNATURES = {
     "topo_oc_noalloc": (_i, [_vp, _vp, _ll, _d, _d, _d, _vp, C.POINTER(_i), _vp]),
     "topo_field_stats": (_i, [_vp, _vp, _ll, C.POINTER(_d), _vp]),
     "topo_gmg_info": (_i, [_vp, C.POINTER(_ll), C.POINTER(_d), C.POINTER(_i)]),
+    "topo_setup_phases": (_i, [_vp, C.POINTER(_d)]),
     "topo_gmg_level_operator": (_i, [_vp, _i, _vp, _vp]),
     "topo_workspace_bytes": (_ll, [_vp]),
     "topo_launch_count": (_ll, []),

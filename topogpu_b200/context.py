@@ -207,6 +207,13 @@ class TopoContext:
         return {"n_free": list(nf), "lambda_max": list(lam),
                 "coarse_solve": {0: "none", 1: "dense_cholesky", 2: "regularised_cholesky"}.get(kind.value, "?")}
 
+    def setup_phases(self) -> dict:
+        """Device milliseconds of the phases of the last gmg_setup."""
+        ms = (C.c_double * 5)()
+        self._chk(self._lib.topo_setup_phases(self._h, ms), "setup_phases")
+        return dict(zip(("fine_diag_lambda", "coarse_stencils", "coarsest_assembly", "cholesky", "inverse"),
+                        list(ms)))
+
     def level_operator(self, level: int) -> torch.Tensor:
         """FP64 stencil of coarse level ``level`` as a (27, 3, 3, nnodes) tensor."""
         nx, ny, nz = self.nel

@@ -573,75 +573,101 @@ __global__ void k_block_tri_inv(const double* __restrict__ Dt, double* __restric
 //   R    = delta_IJ Id - sum_{k in [max(32J, 32I-band), 32I)} L[32I.., k] W[k, 32J..]
 //   W_IJ = Di_I R
 // Every W read is of rows this CTA wrote in an earlier step (visible after
-// __syncthreads), so the column blocks run independently with no grid sync.
+// __syncthreads), so the column blocks run independently with no grid sync;
+// the chain of column block 0 (nT steps) is the critical path, so each CTA
+// has an SM to itself (about 118 KB of shared memory).
+// The K range of a step is staged in 64-wide chunks (next chunk prefetched
+// into registers). Warp w takes the chunk rows k = w, w+8, ...; lane r keeps
+// row r of the 32x32 partial product (32 accumulators) and reads the W row
+// as broadcast 16-byte loads, so each shared-memory wavefront feeds 32 or
+// more FMAs. The 8 warp partials are summed through shared memory.
 // W goes to W64 (lower part, FP64) and to the apply matrices C64 / C32 as W
-// in the lower triangle and W^T in the strict upper triangle. All three
-// share the row stride ldc. The K-loop stages 32-wide chunks of L and W in
-// shared memory with the next chunk prefetched into registers.
-constexpr int TIT = 256;
-__global__ void __launch_bounds__(TIT) k_tri_inverse(int n, int band, const double* __restrict__ L,
-                                                     const double* __restrict__ Di, double* W64, long long ldc,
-                                                     double* C64, float* C32) {
-  __shared__ double Ls[CNB][CNB + 1];
-  __shared__ __align__(16) double Ws[CNB][CNB + 2];
-  __shared__ double Rs[CNB][CNB + 1];
-  __shared__ double Ds[CNB][CNB + 1];
+// in the lower triangle and W^T in the strict upper triangle, all with row
+// stride ldc.
+constexpr int TIT = 256, TKC = 64;
+struct TriSmem {
+  double Ls[CNB][TKC + 1];
+  double Wc[TKC][CNB];
+  double red[TIT / 32][CNB][CNB + 1];
+  double Rs[CNB][CNB + 1];
+  double Ds[CNB][CNB + 1];
+};
+constexpr size_t TRI_SMEM = sizeof(TriSmem);
+
+__global__ void __launch_bounds__(TIT, 1) k_tri_inverse(int n, int band, const double* __restrict__ L,
+                                                        const double* __restrict__ Di, double* W64, long long ldc,
+                                                        double* C64, float* C32) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  TriSmem& S = *reinterpret_cast<TriSmem*>(smem_raw);
   const int J = blockIdx.x, nT = gridDim.x;
-  const int t = threadIdx.x, r = t >> 3, cq = (t & 7) * 4;
+  const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+  const int r = t >> 3, cq = (t & 7) * 4;
   const int j0 = J * CNB;
-  double pl[4], pw[4];
+  double pl[8], pw[8];
   for (int I = J; I < nT; ++I) {
     const int i0 = I * CNB;
     const int klo = max(j0, i0 - band);
     auto fetch = [&](int k0) {
 #pragma unroll
-      for (int m = 0; m < 4; ++m) {
-        const int q = t + TIT * m, hi = q >> 5, lo = q & 31;
-        const int i = i0 + hi, k = k0 + lo;
+      for (int m = 0; m < 8; ++m) {
+        const int q = t + TIT * m;
+        const int i = i0 + (q >> 6), k = k0 + (q & 63);
         pl[m] = (i < n && k < i0) ? L[(long long)i * n + k] : 0.0;
-        const int kw = k0 + hi, cw = j0 + lo;
+        const int kw = k0 + (q >> 5), cw = j0 + (q & 31);
         pw[m] = (kw < i0 && cw < n && cw <= kw) ? W64[(long long)kw * ldc + cw] : 0.0;
       }
     };
-    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    double acc[CNB];
+#pragma unroll
+    for (int c = 0; c < CNB; ++c) acc[c] = 0.0;
     if (klo < i0) fetch(klo);
-    for (int k0 = klo; k0 < i0; k0 += CNB) {
+    for (int k0 = klo; k0 < i0; k0 += TKC) {
       __syncthreads();
 #pragma unroll
-      for (int m = 0; m < 4; ++m) {
+      for (int m = 0; m < 8; ++m) {
         const int q = t + TIT * m;
-        Ls[q >> 5][q & 31] = pl[m];
-        Ws[q >> 5][q & 31] = pw[m];
+        S.Ls[q >> 6][q & 63] = pl[m];
+        S.Wc[q >> 5][q & 31] = pw[m];
       }
       __syncthreads();
-      if (k0 + CNB < i0) fetch(k0 + CNB);
-#pragma unroll 8
-      for (int kk = 0; kk < CNB; ++kk) {
-        const double a = Ls[r][kk];
-        const double2 w01 = *reinterpret_cast<const double2*>(&Ws[kk][cq]);
-        const double2 w23 = *reinterpret_cast<const double2*>(&Ws[kk][cq + 2]);
-        acc[0] = fma(a, w01.x, acc[0]);
-        acc[1] = fma(a, w01.y, acc[1]);
-        acc[2] = fma(a, w23.x, acc[2]);
-        acc[3] = fma(a, w23.y, acc[3]);
+      if (k0 + TKC < i0) fetch(k0 + TKC);
+#pragma unroll 2
+      for (int m = 0; m < TKC / 8; ++m) {
+        const int kk = warp + 8 * m;
+        const double a = S.Ls[lane][kk];
+        const double2* wr = reinterpret_cast<const double2*>(&S.Wc[kk][0]);
+#pragma unroll
+        for (int c2 = 0; c2 < CNB / 2; ++c2) {
+          const double2 w = wr[c2];
+          acc[2 * c2] = fma(a, w.x, acc[2 * c2]);
+          acc[2 * c2 + 1] = fma(a, w.y, acc[2 * c2 + 1]);
+        }
       }
     }
-    for (int q = t; q < CNB * CNB; q += TIT) Ds[q >> 5][q & 31] = Di[(long long)I * CNB * CNB + q];
 #pragma unroll
-    for (int q = 0; q < 4; ++q) Rs[r][cq + q] = ((i0 + r == j0 + cq + q) ? 1.0 : 0.0) - acc[q];
+    for (int c = 0; c < CNB; ++c) S.red[warp][lane][c] = acc[c];
+    for (int q = t; q < CNB * CNB; q += TIT) S.Ds[q >> 5][q & 31] = Di[(long long)I * CNB * CNB + q];
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      double v = (i0 + r == j0 + cq + q) ? 1.0 : 0.0;
+#pragma unroll
+      for (int w = 0; w < TIT / 32; ++w) v -= S.red[w][r][cq + q];
+      S.Rs[r][cq + q] = v;
+    }
     __syncthreads();
     double w[4] = {0.0, 0.0, 0.0, 0.0};
     for (int m = 0; m <= r; ++m) {
-      const double d = Ds[r][m];
+      const double d = S.Ds[r][m];
 #pragma unroll
-      for (int q = 0; q < 4; ++q) w[q] = fma(d, Rs[m][cq + q], w[q]);
+      for (int q = 0; q < 4; ++q) w[q] = fma(d, S.Rs[m][cq + q], w[q]);
     }
     __syncthreads();
     const int i = i0 + r;
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
       const int c = j0 + cq + q;
-      Rs[r][cq + q] = w[q];
+      S.Rs[r][cq + q] = w[q];
       if (i < n && c < n && c <= i) {
         W64[(long long)i * ldc + c] = w[q];
         if (C64 != nullptr && C64 != W64) C64[(long long)i * ldc + c] = w[q];
@@ -656,7 +682,7 @@ __global__ void __launch_bounds__(TIT) k_tri_inverse(int n, int band, const doub
       for (int q = 0; q < 4; ++q) {
         const int ic = i0 + cq + q;
         if (cr < n && ic < n && ic > cr) {
-          const double v = Rs[cq + q][r];
+          const double v = S.Rs[cq + q][r];
           if (C64 != nullptr) C64[(long long)cr * ldc + ic] = v;
           if (C32 != nullptr) C32[(long long)cr * ldc + ic] = (float)v;
         }
@@ -690,7 +716,12 @@ void dense_inverse_factor(int n, int band, const double* A, const double* Dt, do
   const int nT = (n + CNB - 1) / CNB;
   k_block_tri_inv<<<nT, CNB, 0, s>>>(Dt, Di);
   TOPO_LAUNCH_CHECK();
-  k_tri_inverse<<<nT, TIT, 0, s>>>(n, band, A, Di, W64, ldc, C64, C32);
+  static bool attr = false;
+  if (!attr) {
+    TOPO_CUDA_CHECK(cudaFuncSetAttribute(k_tri_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TRI_SMEM));
+    attr = true;
+  }
+  k_tri_inverse<<<nT, TIT, TRI_SMEM, s>>>(n, band, A, Di, W64, ldc, C64, C32);
   TOPO_LAUNCH_CHECK();
 }
 

@@ -173,6 +173,8 @@ struct topo_ctx {
   double* Hs = nullptr;
   cudaStream_t cs = nullptr;
   cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+  cudaEvent_t ev_ph[6] = {};     // setup phase marks (timed)
+  double setup_ms[5] = {0, 0, 0, 0, 0};
   std::vector<void*> allocs;
   long long bytes = 0;
   std::string err;
@@ -422,6 +424,7 @@ void host_galerkin_q(const double* KE, double* Q) {
 void do_setup(topo_ctx* c, const double* E, cudaStream_t s) {
   Level& L0 = c->L[0];
   const long long ne = L0.g.nelem;
+  TOPO_CUDA_CHECK(cudaEventRecord(c->ev_ph[0], s));
   TOPO_CUDA_CHECK(cudaMemcpyAsync(c->E64, E, sizeof(double) * ne, cudaMemcpyDeviceToDevice, s));
   vcast(ne, c->E64, true, c->E32, false, s);
   // level-0 Jacobi diagonal (multigrid_v4.py:684-686)
@@ -440,6 +443,7 @@ void do_setup(topo_ctx* c, const double* E, cudaStream_t s) {
     L0.lam = lambda_fine(c, s);
     c->lam_Emax = Emax;
   }
+  TOPO_CUDA_CHECK(cudaEventRecord(c->ev_ph[1], s));
   for (int l = 1; l < c->n_levels; ++l) {
     Level& Lv = c->L[l];
     if (l == 1) level1_assemble(c->L[0].g, Lv.g, c->E64, Lv.mask, Lv.S64, s);
@@ -453,11 +457,15 @@ void do_setup(topo_ctx* c, const double* E, cudaStream_t s) {
   }
   // coarsest: dense FP64 Cholesky with the reference's eps*I retry (multigrid_v4.py:778-811)
   c->C.kind = 0;
+  TOPO_CUDA_CHECK(cudaEventRecord(c->ev_ph[2], s));
+  TOPO_CUDA_CHECK(cudaEventRecord(c->ev_ph[3], s));
+  TOPO_CUDA_CHECK(cudaEventRecord(c->ev_ph[4], s));
   if (c->n_levels > 1 && c->C.n > 0) {
     const int l = c->n_levels - 1;
     Level& Lc = c->L[l];
     const int n = c->C.n;
     dense_assemble(Lc.g, Lc.S64, c->C.dof_index, n, c->C.A, s);
+    TOPO_CUDA_CHECK(cudaEventRecord(c->ev_ph[3], s));
     int bad = dense_cholesky(n, c->C.band, c->C.A, c->C.Dt, c->C.flag, s);
     if (bad) {
       dense_assemble(Lc.g, Lc.S64, c->C.dof_index, n, c->C.A, s);
@@ -475,10 +483,17 @@ void do_setup(topo_ctx* c, const double* E, cudaStream_t s) {
     } else {
       c->C.kind = 1;
     }
+    TOPO_CUDA_CHECK(cudaEventRecord(c->ev_ph[4], s));
     dense_inverse_factor(n, c->C.band, c->C.A, c->C.Dt, c->C.Di, c->C.work, c->C.ldc,
                          c->vec64 ? c->C.work : nullptr, c->vec64 ? nullptr : c->C.X32, s);
   }
+  TOPO_CUDA_CHECK(cudaEventRecord(c->ev_ph[5], s));
   TOPO_CUDA_CHECK(cudaStreamSynchronize(s));
+  for (int p = 0; p < 5; ++p) {
+    float ms = 0.f;
+    TOPO_CUDA_CHECK(cudaEventElapsedTime(&ms, c->ev_ph[p], c->ev_ph[p + 1]));
+    c->setup_ms[p] = ms;
+  }
   c->setup_done = true;
 }
 
@@ -722,6 +737,7 @@ int topo_ctx_create(int nelx, int nely, int nelz, int n_levels, int mode, int fi
     TOPO_CUDA_CHECK(cudaStreamCreateWithFlags(&c->cs, cudaStreamNonBlocking));
     TOPO_CUDA_CHECK(cudaEventCreateWithFlags(&c->ev_in, cudaEventDisableTiming));
     TOPO_CUDA_CHECK(cudaEventCreateWithFlags(&c->ev_out, cudaEventDisableTiming));
+    for (auto& e : c->ev_ph) TOPO_CUDA_CHECK(cudaEventCreate(&e));
     int nx = nelx, ny = nely, nz = nelz;
     for (int l = 0; l < n_levels; ++l) {
       Level Lv;
@@ -800,6 +816,8 @@ int topo_ctx_destroy(topo_ctx* c) {
   if (c->h_st) cudaFreeHost(c->h_st);
   if (c->ev_in) cudaEventDestroy(c->ev_in);
   if (c->ev_out) cudaEventDestroy(c->ev_out);
+  for (auto& e : c->ev_ph)
+    if (e) cudaEventDestroy(e);
   if (c->cs) cudaStreamDestroy(c->cs);
   delete c;
   return 0;
@@ -1082,6 +1100,16 @@ int topo_gmg_info(topo_ctx* c, long long* n_free, double* lambda_max, int* coars
       if (lambda_max) lambda_max[l] = c->L[l].lam;
     }
     if (coarse_kind) *coarse_kind = c->C.kind;
+    return 0;
+  } catch (const std::exception& e) {
+    return fail(c, e);
+  }
+}
+
+int topo_setup_phases(topo_ctx* c, double* ms) {
+  try {
+    if (!c || !ms) throw std::invalid_argument("topo_setup_phases: null pointer");
+    for (int p = 0; p < 5; ++p) ms[p] = c->setup_ms[p];
     return 0;
   } catch (const std::exception& e) {
     return fail(c, e);

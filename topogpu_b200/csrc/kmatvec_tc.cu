@@ -2,8 +2,8 @@
 // cores (FP32 accumulation in tensor memory), for the mixed-precision smoother
 // and the BF16 operator entry point.
 //
-// Per CTA: a patch of 16 x 16 elements in (x, y) and a chunk of z layers.
-// For every element layer the contraction Y_e = KE u_e of 256 elements is
+// Work items: patches of 16 x 16 elements in (x, y) times z layers, walked by
+// persistent CTAs (pipeline below). For every element layer the contraction Y_e = KE u_e of 256 elements is
 // four tcgen05.mma (M=128 elements, N=32 outputs, K=16 inputs each):
 //   * the nodal values of two z planes sit in shared memory as BF16 records
 //     (ux, uy, uz, 0) ordered x-fastest; an element's 32-entry input row is
@@ -36,34 +36,16 @@ namespace tc {
 constexpr int PX = 16, PY = 16;       // elements per patch in x and y
 constexpr int OWN = 15;               // owned nodes per patch per direction
 constexpr int ZB = 4;                 // element layers per tensor-memory block
-constexpr int ZC = 16;                // element layers per CTA
 constexpr int RX = 16;                // node slots per row (x), 8 bytes each
 constexpr int RY = 17;                // node rows per plane (y)
 constexpr int NPL = ZB + 1;           // node planes per block
 constexpr int ROW_B = RX * 8;         // 128 bytes
 constexpr int PLANE_B = RX * RY * 8;  // 2176 bytes
 constexpr int COPY_B = NPL * PLANE_B; // 10880 bytes
-constexpr int NT = 128;
-constexpr uint32_t TMEM_COLS = 256;   // ZB layers x 2 parity tiles x 32 columns
 constexpr int NLEV = ZB + 1;          // output node levels staged per block
-
-// shared-memory layout (bytes, from a 1024-aligned base; every region 16-aligned)
-constexpr int al16(int x) { return (x + 15) & ~15; }
-constexpr int OFF_B = 0;                                 // B operand: 32 x 32 bf16 = 2048
-constexpr int OFF_A0 = 2048;                             // node copy, even x
-constexpr int OFF_A1 = OFF_A0 + COPY_B;                  // node copy, odd x
-constexpr int OFF_E = al16(OFF_A1 + COPY_B);             // E: ZB x 16 x 16 floats
-constexpr int OFF_OUT = al16(OFF_E + ZB * PY * PX * 4);  // staged outputs
 constexpr int OUT_FLOATS = OWN * OWN * NLEV * 3;
-constexpr int OFF_XCH = al16(OFF_OUT + OUT_FLOATS * 4);  // warp hand-off: 4 x 8 x 12 floats
-constexpr int OFF_BAR = al16(OFF_XCH + 4 * 8 * 12 * 4);  // ZB mbarriers (8-byte objects)
-constexpr int OFF_TMEM = al16(OFF_BAR + ZB * 8);         // tensor-memory base address
-static_assert(OFF_BAR % 8 == 0 && OFF_TMEM % 4 == 0, "barrier alignment");
-constexpr int SMEM_BYTES = OFF_TMEM + 16 + 1024;  // + alignment slack
-// 100 KB requested so that at most two CTAs share an SM (2 x 256 TMEM columns).
-constexpr int SMEM_REQUEST = 100 * 1024;
-static_assert(SMEM_BYTES <= SMEM_REQUEST, "shared memory budget");
-static_assert(OFF_A0 % 16 == 0 && OFF_A1 % 16 == 0 && PLANE_B % 16 == 0, "descriptor alignment");
+constexpr int al16(int x) { return (x + 15) & ~15; }
+static_assert(PLANE_B % 16 == 0, "descriptor alignment");
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return (uint32_t)__cvta_generic_to_shared(p);
@@ -153,202 +135,368 @@ __device__ __forceinline__ float ldu(const TU* p) {
   else return (float)*p;
 }
 
+// ---------------------------------------------------------------------------
+// Persistent warp-specialised pipeline. One CTA per SM walks a contiguous
+// range of (column, z-layer) items, column = one 16x16-element patch, in
+// blocks of ZB layers; four roles overlap successive blocks:
+//   load   (warps 8-11): node planes -> BF16 records in a 3-stage ring
+//   mma    (warp 12, one thread): 4 tcgen05.mma per layer into one of two
+//          256-column TMEM buffers, commit -> tfull[tb] and empty[s]
+//   reduce (warps 0-3 = TMEM lanes 0-127): TMEM -> E scaling -> nodal sums
+//          (x pair in registers, y by shuffles, z by a carried share) ->
+//          staged outputs (two buffers)
+//   store  (warps 4-7): the epilogue (Store / Residual / RUpd / ChebR) on the
+//          owned nodes of the block, z-contiguous
+// Every wait is an mbarrier poll with an iteration limit; a timeout raises
+// the device error flag and a CTA-wide abort so the other roles stop too.
+constexpr int NSTAGE = 3;
+constexpr int STAGE_B = 2 * COPY_B;
+constexpr int OUT_B = al16(OUT_FLOATS * 4);
+constexpr int NT2 = 416;
+constexpr int W_STORE = 4, W_LOAD = 8, W_MMA = 12;
+constexpr int P_B = 0;
+constexpr int P_ST = 2048;
+constexpr int P_OUT = al16(P_ST + NSTAGE * STAGE_B);
+constexpr int P_XCH = al16(P_OUT + 2 * OUT_B);
+constexpr int P_BAR = al16(P_XCH + 4 * 8 * 12 * 4);
+constexpr int NBAR = 2 * NSTAGE + 8;  // full[3] empty[3] tfull[2] tempty[2] ofull[2] oempty[2]
+constexpr int P_TMEM = al16(P_BAR + NBAR * 8);
+constexpr int P_ABORT = P_TMEM + 4;
+constexpr int SMEM2_BYTES = P_ABORT + 4 + 1024;
+constexpr int SMEM2_REQUEST = 120 * 1024;  // one CTA per SM: it owns all 512 TMEM columns
+constexpr uint32_t TMEM2_COLS = 512;
+static_assert(SMEM2_BYTES <= SMEM2_REQUEST, "shared memory budget");
+static_assert(P_ST % 16 == 0 && STAGE_B % 16 == 0 && COPY_B % 16 == 0, "descriptor alignment");
+static_assert(P_BAR % 8 == 0, "barrier alignment");
+
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+// Bounded wait that also gives up when another role has aborted.
+__device__ __forceinline__ bool wait_bar(uint32_t bar, uint32_t parity, volatile int* abort_flag, int* errflag) {
+  for (int it = 0; it < (1 << 22); ++it) {
+    if (mbar_try(bar, parity)) return true;
+    if ((it & 31) == 31 && *abort_flag) return false;
+  }
+  *abort_flag = 1;
+  atomicExch(errflag, 1);
+  return false;
+}
+
+// AND of a predicate over the 128 reduce threads (named barrier 1): their
+// decision to stop must be uniform because they meet at that barrier.
+__device__ __forceinline__ bool all_reduce_threads(bool pred) {
+  uint32_t r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\t"
+      "setp.ne.u32 p, %1, 0;\n\t"
+      "bar.red.and.pred q, 1, 128, p;\n\t"
+      "selp.u32 %0, 1, 0, q;\n\t}\n"
+      : "=r"(r)
+      : "r"((uint32_t)pred)
+      : "memory");
+  return r != 0;
+}
+
+// The block sequence of one CTA: layer items [lo, hi) in column-major order
+// (item = column * nz + z); per column a segment [z0, z1) processed from the
+// seed layer max(0, z0 - 1) in blocks of ZB layers.
+struct BlockSeq {
+  int nz, lo, hi, c, c_hi, zb, z0, z1;
+  __device__ void seg() {
+    z0 = (c == lo / nz) ? lo - c * nz : 0;
+    z1 = (c == c_hi) ? hi - c * nz : nz;
+    zb = max(0, z0 - 1);
+  }
+  __device__ void init(int nz_, int lo_, int hi_) {
+    nz = nz_, lo = lo_, hi = hi_;
+    c = lo / nz;
+    c_hi = (hi - 1) / nz;
+    if (lo < hi) seg();
+    else c = c_hi + 1;
+  }
+  __device__ bool valid() const { return lo < hi && c <= c_hi; }
+  __device__ int nb() const { return min(ZB, z1 - zb); }
+  __device__ bool first() const { return zb == max(0, z0 - 1); }
+  __device__ void next() {
+    zb += ZB;
+    if (zb >= z1) {
+      ++c;
+      if (c <= c_hi) seg();
+    }
+  }
+};
+
 // q(dx,dy,dz) = dx + 2 dy + 4 dz indexes the 8 corners; output column q*4+c.
 template <typename TU, Epi EPI>
-__global__ void __launch_bounds__(NT, 2)
+__global__ void __launch_bounds__(NT2, 1)
 k_level0_tc(Grid g, const TU* __restrict__ u, const float* __restrict__ E, const uint8_t* __restrict__ mask,
-            const __nv_bfloat16* __restrict__ Bglob, EpiDev<float> ep, const KrylovState* st, int* errflag) {
+            const __nv_bfloat16* __restrict__ Bglob, EpiDev<float> ep, const KrylovState* st, int* errflag,
+            int ncoly) {
   if (st != nullptr && st->done) return;
   extern __shared__ unsigned char smem_raw[];
   unsigned char* sm = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int x0 = -1 + OWN * (int)blockIdx.x, y0 = -1 + OWN * (int)blockIdx.y;
-  const int zc0 = ZC * (int)blockIdx.z;
-  const int zc1 = min(g.nz, zc0 + ZC);
-  const int zs = max(0, zc0 - 1);  // one extra layer to seed the z carry
+  const uint32_t bar_full = smem_u32(sm + P_BAR), bar_empty = bar_full + 8 * NSTAGE;
+  const uint32_t bar_tfull = bar_empty + 8 * NSTAGE, bar_tempty = bar_tfull + 16;
+  const uint32_t bar_ofull = bar_tempty + 16, bar_oempty = bar_ofull + 16;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm + P_TMEM);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(sm + P_ABORT);
 
-  float* es = reinterpret_cast<float*>(sm + OFF_E);
-  float* outs = reinterpret_cast<float*>(sm + OFF_OUT);
-  float* xch = reinterpret_cast<float*>(sm + OFF_XCH);
-  const uint32_t bar0 = smem_u32(sm + OFF_BAR);
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm + OFF_TMEM);
-
-  // B operand into its canonical K-major layout (precomputed on the host)
-  for (int i = tid; i < 1024 / 8; i += NT)
-    reinterpret_cast<uint4*>(sm + OFF_B)[i] = reinterpret_cast<const uint4*>(Bglob)[i];
-  if (tid == 0)
-    for (int l = 0; l < ZB; ++l) mbar_init(bar0 + 8 * l, 1);
-  if (warp == 0) {
+  for (int i = tid; i < 1024 / 8; i += NT2)
+    reinterpret_cast<uint4*>(sm + P_B)[i] = reinterpret_cast<const uint4*>(Bglob)[i];
+  if (tid == 0) {
+    for (int s = 0; s < NSTAGE; ++s) {
+      mbar_init(bar_full + 8 * s, 128);
+      mbar_init(bar_empty + 8 * s, 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(bar_tfull + 8 * b, 1);
+      mbar_init(bar_tempty + 8 * b, 128);
+      mbar_init(bar_ofull + 8 * b, 128);
+      mbar_init(bar_oempty + 8 * b, 128);
+    }
+    *abort_flag = 0;
+  }
+  if (warp == W_MMA) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                 "r"(TMEM_COLS));
+                 "r"(TMEM2_COLS));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  fence_async_smem();
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tbase = *tmem_slot;
 
-  // thread <-> element pair: TMEM lane m = 32 warp + lane = 8 gy + r
-  const int m = tid;
-  const int gy = m >> 3, r = m & 7;
-  float carry[2][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
-  uint32_t phase = 0;
-  bool ok = true;
+  const int ncol = ((g.NX + OWN - 1) / OWN) * ncoly;
+  const long long T = (long long)ncol * g.nz;
+  const int lo = (int)(T * blockIdx.x / gridDim.x), hi = (int)(T * (blockIdx.x + 1) / gridDim.x);
+  BlockSeq q;
+  q.init(g.nz, lo, hi);
 
-  for (int zb = zs; zb < zc1 && ok; zb += ZB) {
-    const int nb = min(ZB, zc1 - zb);
-    // ---- stage node planes zb..zb+nb (BF16 records) and moduli ----------
-    for (int idx = tid; idx < (nb + 1) * 17 * 17; idx += NT) {
-      const int pz = idx % (nb + 1);
-      const int col = idx / (nb + 1);
-      const int xs = col % 17, ys = col / 17;
-      const int gx = x0 + xs, gyy = y0 + ys, gz = zb + pz;
-      float a = 0.f, b = 0.f, c = 0.f;
-      if (gx >= 0 && gx < g.NX && gyy >= 0 && gyy < g.NY && gz < g.NZ) {
-        const long long n = ((long long)gx * g.NY + gyy) * g.NZ + gz;
-        a = ldu(u + 3 * n);
-        b = ldu(u + 3 * n + 1);
-        c = ldu(u + 3 * n + 2);
+  if (warp >= W_LOAD && warp < W_MMA) {
+    // ------------------------------------------------------------ load
+    const int pt = tid - 32 * W_LOAD;
+    for (int k = 0; q.valid(); ++k, q.next()) {
+      const int s = k % NSTAGE;
+      if (!wait_bar(bar_empty + 8 * s, ((k / NSTAGE) & 1) ^ 1, abort_flag, errflag)) break;
+      const int x0 = -1 + OWN * (q.c / ncoly), y0 = -1 + OWN * (q.c % ncoly);
+      const int zb = q.zb, nb = q.nb();
+      unsigned char* A0 = sm + P_ST + s * STAGE_B;
+      unsigned char* A1 = A0 + COPY_B;
+      for (int cidx = pt; cidx < 17 * 17; cidx += 128) {
+        const int xs = cidx % 17, ys = cidx / 17;
+        const int gx = x0 + xs, gyy = y0 + ys;
+        const bool in = gx >= 0 && gx < g.NX && gyy >= 0 && gyy < g.NY;
+        const long long n0 = ((long long)gx * g.NY + gyy) * g.NZ + zb;
+        float v[ZB + 1][3];
+#pragma unroll
+        for (int pz = 0; pz <= ZB; ++pz)
+#pragma unroll
+          for (int c = 0; c < 3; ++c) v[pz][c] = (in && pz <= nb) ? ldu(u + 3 * (n0 + pz) + c) : 0.f;
+#pragma unroll
+        for (int pz = 0; pz <= ZB; ++pz) {
+          const uint2 rec = pack_node(v[pz][0], v[pz][1], v[pz][2]);
+          if (xs < RX) *reinterpret_cast<uint2*>(A0 + pz * PLANE_B + ys * ROW_B + xs * 8) = rec;
+          if (xs >= 1) *reinterpret_cast<uint2*>(A1 + pz * PLANE_B + ys * ROW_B + (xs - 1) * 8) = rec;
+        }
       }
-      const uint2 rec = pack_node(a, b, c);
-      if (ys < RY) {
-        if (xs < RX) *reinterpret_cast<uint2*>(sm + OFF_A0 + pz * PLANE_B + ys * ROW_B + xs * 8) = rec;
-        if (xs >= 1) *reinterpret_cast<uint2*>(sm + OFF_A1 + pz * PLANE_B + ys * ROW_B + (xs - 1) * 8) = rec;
+      fence_async_smem();
+      mbar_arrive(bar_full + 8 * s);
+    }
+  } else if (warp == W_MMA) {
+    // ------------------------------------------------------------- mma
+    if (lane == 0) {
+      int last = -1;
+      for (int k = 0; q.valid(); ++k, q.next()) {
+        const int s = k % NSTAGE, tb = k & 1;
+        if (!wait_bar(bar_full + 8 * s, (k / NSTAGE) & 1, abort_flag, errflag)) break;
+        if (!wait_bar(bar_tempty + 8 * tb, ((k >> 1) & 1) ^ 1, abort_flag, errflag)) break;
+        tc_fence_after();
+        const uint32_t a0 = smem_u32(sm + P_ST + s * STAGE_B), a1 = a0 + COPY_B, bb = smem_u32(sm + P_B);
+        const int nb = q.nb();
+        for (int l = 0; l < nb; ++l)
+#pragma unroll
+          for (int p = 0; p < 2; ++p)
+#pragma unroll
+            for (int kh = 0; kh < 2; ++kh) {
+              const uint32_t abase = (p ? a1 : a0) + (l + kh) * PLANE_B;
+              mma_bf16(tbase + tb * 256 + l * 64 + p * 32, make_desc(abase, ROW_B, ROW_B),
+                       make_desc(bb + kh * 256, 128, 512), kh);
+            }
+        mma_commit(bar_tfull + 8 * tb);
+        mma_commit(bar_empty + 8 * s);
+        last = k;
+      }
+      // never leave MMAs in flight behind an abort (bounded, ignores the abort flag)
+      if (last >= 0) {
+        const uint32_t b = bar_tfull + 8 * (last & 1), par = (last >> 1) & 1;
+        for (int it = 0; it < (1 << 22) && !mbar_try(b, par); ++it) {
+        }
       }
     }
-    for (int idx = tid; idx < nb * PY * PX; idx += NT) {
-      const int l = idx / (PY * PX), rem = idx % (PY * PX);
-      const int ys = rem / PX, xs = rem % PX;
-      const int ex = x0 + xs, ey = y0 + ys, ez = zb + l;
-      float v = 0.f;
-      if (ex >= 0 && ex < g.nx && ey >= 0 && ey < g.ny) v = E[((long long)ex * g.ny + ey) * g.nz + ez];
-      es[idx] = v;
-    }
-    fence_async_smem();
-    tc_fence_before();
-    __syncthreads();
-    // ---- tensor cores: 2 parity tiles x 2 K halves per layer --------------
-    if (tid == 0) {
+  } else if (warp < W_STORE) {
+    // ---------------------------------------------------------- reduce
+    const int m = tid, gy = m >> 3, r = m & 7;
+    float* xch = reinterpret_cast<float*>(sm + P_XCH);
+    float carry[2][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
+    for (int k = 0; q.valid(); ++k, q.next()) {
+      const int tb = k & 1, ob = k & 1;
+      const int x0 = -1 + OWN * (q.c / ncoly), y0 = -1 + OWN * (q.c % ncoly);
+      const int zb = q.zb, nb = q.nb(), z0 = q.z0, z1 = q.z1;
+      if (q.first()) {
+#pragma unroll
+        for (int nd = 0; nd < 2; ++nd)
+#pragma unroll
+          for (int c = 0; c < 3; ++c) carry[nd][c] = 0.f;
+      }
+      // moduli of this thread's two elements, fetched before the wait
+      float EA[ZB], EB[ZB];
+      const int ex = x0 + 2 * r, ey = y0 + gy;
+      const bool yin = ey >= 0 && ey < g.ny;
+#pragma unroll
+      for (int l = 0; l < ZB; ++l) {
+        const long long e0 = ((long long)ex * g.ny + ey) * g.nz + zb + l;
+        EA[l] = (l < nb && yin && ex >= 0 && ex < g.nx) ? E[e0] : 0.f;
+        EB[l] = (l < nb && yin && ex + 1 >= 0 && ex + 1 < g.nx) ? E[e0 + (long long)g.ny * g.nz] : 0.f;
+      }
+      bool ok = wait_bar(bar_tfull + 8 * tb, (k >> 1) & 1, abort_flag, errflag);
+      ok = ok && wait_bar(bar_oempty + 8 * ob, ((k >> 1) & 1) ^ 1, abort_flag, errflag);
+      if (!all_reduce_threads(ok)) break;
       tc_fence_after();
-      const uint32_t a0 = smem_u32(sm + OFF_A0), a1 = smem_u32(sm + OFF_A1), bb = smem_u32(sm + OFF_B);
-      for (int l = 0; l < nb; ++l) {
+      float* outs = reinterpret_cast<float*>(sm + P_OUT + ob * OUT_B);
 #pragma unroll
-        for (int p = 0; p < 2; ++p)
+      for (int l = 0; l < ZB; ++l) {
+        if (l >= nb) break;
+        const int z = zb + l;
+        float OA[32], OB[32];
+        const uint32_t tl = tbase + ((uint32_t)(warp * 32) << 16) + tb * 256 + l * 64;
+        tmem_ld32(tl, OA);
+        tmem_ld32(tl + 32, OB);
+        tmem_wait_ld();
+        // S[node][dy][dz][c]: node 0 = x 2r+1 (shared by A and B), node 1 = x 2r+2
+        float S[2][2][2][3];
 #pragma unroll
-          for (int kh = 0; kh < 2; ++kh) {
-            const uint32_t abase = (p ? a1 : a0) + (l + kh) * PLANE_B;
-            mma_bf16(tbase + l * 64 + p * 32, make_desc(abase, ROW_B, ROW_B), make_desc(bb + kh * 256, 128, 512),
-                     kh);
-          }
-        mma_commit(bar0 + 8 * l);
-      }
-    }
-    // ---- epilogue: layer by layer ------------------------------------------
-    for (int l = 0; l < nb; ++l) {
-      const int z = zb + l;
-      if (!mbar_wait(bar0 + 8 * l, phase)) {
-        ok = false;
-        if (tid == 0) atomicExch(errflag, 1);
-      }
-      tc_fence_after();
-      float OA[32], OB[32];
-      const uint32_t tl = tbase + ((uint32_t)(warp * 32) << 16) + l * 64;
-      tmem_ld32(tl, OA);
-      tmem_ld32(tl + 32, OB);
-      tmem_wait_ld();
-      const float EA = es[l * PY * PX + gy * PX + 2 * r];
-      const float EB = es[l * PY * PX + gy * PX + 2 * r + 1];
-      // S[node][dy][dz][c]: node 0 = x 2r+1 (shared by A and B), node 1 = x 2r+2
-      float S[2][2][2][3];
+        for (int dy = 0; dy < 2; ++dy)
 #pragma unroll
-      for (int dy = 0; dy < 2; ++dy)
+          for (int dz = 0; dz < 2; ++dz)
 #pragma unroll
-        for (int dz = 0; dz < 2; ++dz)
+            for (int c = 0; c < 3; ++c) {
+              const int q0 = 0 + 2 * dy + 4 * dz, q1 = 1 + 2 * dy + 4 * dz;
+              const float a_lo = EA[l] * OA[q0 * 4 + c];
+              const float a_hi = EA[l] * OA[q1 * 4 + c];
+              const float b_lo = EB[l] * OB[q0 * 4 + c];
+              const float b_hi = EB[l] * OB[q1 * 4 + c];
+              const float next_a_lo = __shfl_down_sync(0xffffffffu, a_lo, 1);
+              S[0][dy][dz][c] = a_hi + b_lo;
+              S[1][dy][dz][c] = b_hi + next_a_lo;
+            }
+        if (lane >= 24) {
+          float* xo = xch + (warp * 8 + (lane - 24)) * 12;
 #pragma unroll
-          for (int c = 0; c < 3; ++c) {
-            const int q0 = 0 + 2 * dy + 4 * dz, q1 = 1 + 2 * dy + 4 * dz;
-            const float a_lo = EA * OA[q0 * 4 + c];  // A's corner at x 2r (dx=0)
-            const float a_hi = EA * OA[q1 * 4 + c];  // A's corner at x 2r+1
-            const float b_lo = EB * OB[q0 * 4 + c];  // B's corner at x 2r+1
-            const float b_hi = EB * OB[q1 * 4 + c];  // B's corner at x 2r+2
-            const float next_a_lo = __shfl_down_sync(0xffffffffu, a_lo, 1);  // lane+1's A corner at x 2r+2
-            S[0][dy][dz][c] = a_hi + b_lo;
-            S[1][dy][dz][c] = b_hi + next_a_lo;
-          }
-      // y: node row gy takes dy=0 from element row gy and dy=1 from row gy-1
-      if (lane >= 24) {
-        float* xo = xch + (warp * 8 + (lane - 24)) * 12;
+          for (int nd = 0; nd < 2; ++nd)
+#pragma unroll
+            for (int dz = 0; dz < 2; ++dz)
+#pragma unroll
+              for (int c = 0; c < 3; ++c) xo[(nd * 2 + dz) * 3 + c] = S[nd][1][dz][c];
+        }
+        asm volatile("bar.sync 1, 128;" ::: "memory");
+        float U[2][2][3];
 #pragma unroll
         for (int nd = 0; nd < 2; ++nd)
 #pragma unroll
           for (int dz = 0; dz < 2; ++dz)
 #pragma unroll
-            for (int c = 0; c < 3; ++c) xo[(nd * 2 + dz) * 3 + c] = S[nd][1][dz][c];
-      }
-      asm volatile("bar.sync 1, 128;" ::: "memory");
-      float U[2][2][3];
+            for (int c = 0; c < 3; ++c) {
+              float prev = __shfl_up_sync(0xffffffffu, S[nd][1][dz][c], 8);
+              if (lane < 8) prev = (warp > 0) ? xch[((warp - 1) * 8 + lane) * 12 + (nd * 2 + dz) * 3 + c] : 0.f;
+              U[nd][dz][c] = S[nd][0][dz][c] + prev;
+            }
+        const int lev = z - zb;
 #pragma unroll
-      for (int nd = 0; nd < 2; ++nd)
-#pragma unroll
-        for (int dz = 0; dz < 2; ++dz)
+        for (int nd = 0; nd < 2; ++nd) {
+          const int xr = 2 * r + 1 + nd;
+          const bool own = xr <= OWN && gy >= 1;
 #pragma unroll
           for (int c = 0; c < 3; ++c) {
-            float prev = __shfl_up_sync(0xffffffffu, S[nd][1][dz][c], 8);
-            if (lane < 8) prev = (warp > 0) ? xch[((warp - 1) * 8 + lane) * 12 + (nd * 2 + dz) * 3 + c] : 0.f;
-            U[nd][dz][c] = S[nd][0][dz][c] + prev;
+            const float v = U[nd][0][c] + carry[nd][c];
+            carry[nd][c] = U[nd][1][c];
+            if (own && z >= z0) outs[(((gy - 1) * OWN + (xr - 1)) * NLEV + lev) * 3 + c] = v;
           }
-      // z: level z = dz0 share of layer z + carried dz1 share of layer z-1
-      const int lev = z - zb;  // staging slot of node level z
+        }
+        asm volatile("bar.sync 1, 128;" ::: "memory");  // xch reuse
+      }
+      tc_fence_before();
+      mbar_arrive(bar_tempty + 8 * tb);
+      if ((zb + nb == z1) && (z1 == g.nz)) {
 #pragma unroll
-      for (int nd = 0; nd < 2; ++nd) {
-        const int xr = 2 * r + 1 + nd;  // node x relative to x0
-        const bool own = xr <= OWN && gy >= 1;
+        for (int nd = 0; nd < 2; ++nd) {
+          const int xr = 2 * r + 1 + nd;
+          if (xr <= OWN && gy >= 1)
 #pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          const float v = U[nd][0][c] + carry[nd][c];
-          carry[nd][c] = U[nd][1][c];
-          if (own && z >= zc0) outs[(((gy - 1) * OWN + (xr - 1)) * NLEV + lev) * 3 + c] = v;
+            for (int c = 0; c < 3; ++c) outs[(((gy - 1) * OWN + (xr - 1)) * NLEV + nb) * 3 + c] = carry[nd][c];
         }
       }
-      asm volatile("bar.sync 1, 128;" ::: "memory");  // xch reuse
+      mbar_arrive(bar_ofull + 8 * ob);
     }
-    // node level zc1 == nz comes from the carry alone
-    const bool last_level = (zb + nb == zc1) && (zc1 == g.nz);
-    if (last_level) {
+  } else {
+    // ----------------------------------------------------------- store
+    const int stid = tid - 32 * W_STORE;
+    for (int k = 0; q.valid(); ++k, q.next()) {
+      const int ob = k & 1;
+      if (!wait_bar(bar_ofull + 8 * ob, (k >> 1) & 1, abort_flag, errflag)) break;
+      const float* outs = reinterpret_cast<const float*>(sm + P_OUT + ob * OUT_B);
+      const int x0 = -1 + OWN * (q.c / ncoly), y0 = -1 + OWN * (q.c % ncoly);
+      const int zb = q.zb, nb = q.nb();
+      const bool last_level = (zb + nb == q.z1) && (q.z1 == g.nz);
+      const int zlo = max(zb, q.z0);
+      const int nlev_out = (zb + nb) - zlo + (last_level ? 1 : 0);
+      if (nlev_out > 0) {
+        const int per_node = nlev_out * 3;
+        const int total = OWN * OWN * per_node;
+        for (int base = stid; base < total; base += 4 * 128) {
+          long long ii[4];
+          float acc[4], ui[4];
+          bool val[4], fr[4];
 #pragma unroll
-      for (int nd = 0; nd < 2; ++nd) {
-        const int xr = 2 * r + 1 + nd;
-        if (xr <= OWN && gy >= 1)
+          for (int j = 0; j < 4; ++j) {
+            const int idx = base + 128 * j;
+            val[j] = false;
+            ii[j] = 0;
+            acc[j] = 0.f;
+            if (idx < total) {
+              const int on = idx / per_node, rem = idx % per_node;
+              const int lv = rem / 3, c = rem % 3;
+              const int xr = on % OWN + 1, yr = on / OWN + 1;
+              const int gx = x0 + xr, gyy = y0 + yr, gz = zlo + lv;
+              if (gx < g.NX && gyy < g.NY && gz < g.NZ) {
+                val[j] = true;
+                ii[j] = 3 * (((long long)gx * g.NY + gyy) * g.NZ + gz) + c;
+                acc[j] = outs[(on * NLEV + (gz - zb)) * 3 + c];
+              }
+            }
+          }
 #pragma unroll
-          for (int c = 0; c < 3; ++c) outs[(((gy - 1) * OWN + (xr - 1)) * NLEV + nb) * 3 + c] = carry[nd][c];
+          for (int j = 0; j < 4; ++j) {
+            fr[j] = val[j] ? mask[ii[j]] != 0 : false;
+            ui[j] = (EPI == Epi::ChebR && val[j]) ? ldu(u + ii[j]) : 0.f;
+          }
+#pragma unroll
+          for (int j = 0; j < 4; ++j)
+            if (val[j]) epilogue_store<float, EPI>(ep, ii[j], fr[j], acc[j], ui[j]);
+        }
       }
+      mbar_arrive(bar_oempty + 8 * ob);
     }
-    phase ^= 1u;
-    tc_fence_before();
-    __syncthreads();
-    // ---- write owned nodes, z-contiguous --------------------------------
-    const int zlo = max(zb, zc0);
-    const int nlev_out = (zb + nb) - zlo + (last_level ? 1 : 0);
-    if (nlev_out > 0) {
-      const int per_node = nlev_out * 3;
-      for (int idx = tid; idx < OWN * OWN * per_node; idx += NT) {
-        const int on = idx / per_node, rem = idx % per_node;
-        const int lv = rem / 3, c = rem % 3;
-        const int xr = on % OWN + 1, yr = on / OWN + 1;
-        const int gx = x0 + xr, gyy = y0 + yr, gz = zlo + lv;
-        if (gx >= g.NX || gyy >= g.NY || gz >= g.NZ) continue;
-        const long long i = 3 * (((long long)gx * g.NY + gyy) * g.NZ + gz) + c;
-        const float acc = outs[(on * NLEV + (gz - zb)) * 3 + c];
-        epilogue_store<float, EPI>(ep, i, mask[i] != 0, acc, ldu(u + i));
-      }
-    }
-    __syncthreads();
   }
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
-  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(TMEM_COLS));
+  if (warp == W_MMA)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(TMEM2_COLS));
 }
 
 }  // namespace tc
@@ -394,16 +542,21 @@ void tc_prepare(const double* KE) {
 template <typename TU, Epi EPI>
 static void launch_tc(const Grid& g, const void* u, const void* E, const uint8_t* mask, void* y, const EpiArgs& ea,
                       cudaStream_t s) {
-  static bool attr_set = false;
-  if (!attr_set) {
+  static int nsm = 0;
+  if (nsm == 0) {
+    int dev = 0;
+    TOPO_CUDA_CHECK(cudaGetDevice(&dev));
+    TOPO_CUDA_CHECK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
     TOPO_CUDA_CHECK(cudaFuncSetAttribute(tc::k_level0_tc<TU, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         tc::SMEM_REQUEST));
-    attr_set = true;
+                                         tc::SMEM2_REQUEST));
   }
-  dim3 grid((g.NX + tc::OWN - 1) / tc::OWN, (g.NY + tc::OWN - 1) / tc::OWN, (g.nz + tc::ZC - 1) / tc::ZC);
+  const int ncolx = (g.NX + tc::OWN - 1) / tc::OWN, ncoly = (g.NY + tc::OWN - 1) / tc::OWN;
+  const long long items = (long long)ncolx * ncoly * g.nz;
+  if (items >= (1LL << 31)) throw std::runtime_error("level0_apply_tc: grid too large");
+  const int grid = (int)std::min<long long>(items, nsm);
   const EpiDev<float> ep = make_epi<float>(y, ea);
-  tc::k_level0_tc<TU, EPI><<<grid, tc::NT, tc::SMEM_REQUEST, s>>>(g, (const TU*)u, (const float*)E, mask, g_tcB, ep,
-                                                                  ea.st, g_tcErr);
+  tc::k_level0_tc<TU, EPI><<<grid, tc::NT2, tc::SMEM2_REQUEST, s>>>(g, (const TU*)u, (const float*)E, mask, g_tcB,
+                                                                   ep, ea.st, g_tcErr, ncoly);
   TOPO_LAUNCH_CHECK();
 }
 
