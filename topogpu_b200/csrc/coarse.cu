@@ -468,44 +468,48 @@ void dense_assemble(const Grid& g, const double* S, const int* dof_index, int n,
 // read as L afterwards.
 constexpr int CNB = 32;
 
-// One panel step. Every CTA factors the (k,k) block in shared memory (the
-// same arithmetic in each, so all agree); CTA 0 stores it in Dt and raises
+// One panel step. In every CTA, warp 0 factors the (k,k) block in registers
+// (lane i holds row i; column j is broadcast with shuffles), the same
+// arithmetic in each CTA so all agree; CTA 0 stores it in Dt and raises
 // `flag` on a non-positive or non-finite pivot (the pivot is then taken as
-// 1). Each thread then solves one panel row i in [k+nb, min(n, k+nb+band)):
-// L_ik L_kk^T = A_ik.
+// 1). Each thread then solves one panel row i in [k+nb, min(n, k+nb+band)),
+// L_ik L_kk^T = A_ik, column by column (the updates of later columns are
+// independent, so they overlap).
 __global__ void k_chol_step(int n, int k, int band, double* __restrict__ A, double* __restrict__ Dt,
                             int* __restrict__ flag) {
   __shared__ double L[CNB][CNB + 1];
   const int nb = min(CNB, n - k);
-  for (int q = threadIdx.x; q < CNB * CNB; q += blockDim.x) {
-    const int i = q / CNB, j = q % CNB;
-    L[i][j] = (i < nb && j < nb) ? A[(long long)(k + i) * n + k + j] : (i == j ? 1.0 : 0.0);
+  if (threadIdx.x < 32) {
+    const int i = threadIdx.x;
+    double a[CNB];
+#pragma unroll
+    for (int c = 0; c < CNB; ++c)
+      a[c] = (i < nb && c < nb && c <= i) ? A[(long long)(k + i) * n + k + c] : (i == c ? 1.0 : 0.0);
+    bool bad = false;
+#pragma unroll
+    for (int j = 0; j < CNB; ++j) {
+      const double d = __shfl_sync(0xffffffffu, a[j], j);
+      const bool ok = d > 0.0 && isfinite(d);
+      bad |= !ok;
+      const double ljj = ok ? sqrt(d) : 1.0;
+      if (i > j) a[j] = a[j] / ljj;
+      else if (i == j) a[j] = ljj;
+#pragma unroll
+      for (int c = j + 1; c < CNB; ++c) {
+        const double lcj = __shfl_sync(0xffffffffu, a[j], c);
+        if (i >= c) a[c] -= a[j] * lcj;
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < CNB; ++c) L[i][c] = (c <= i) ? a[c] : 0.0;
+    if (blockIdx.x == 0) {
+      double* D = Dt + (long long)(k / CNB) * CNB * CNB + i * CNB;
+#pragma unroll
+      for (int c = 0; c < CNB; ++c) D[c] = (c <= i) ? a[c] : 0.0;
+      if (i == 0 && bad) *flag = 1;
+    }
   }
   __syncthreads();
-  bool bad = false;
-  for (int j = 0; j < nb; ++j) {
-    const double d = L[j][j];
-    const bool ok = d > 0.0 && isfinite(d);
-    bad |= !ok;
-    const double ljj = ok ? sqrt(d) : 1.0;
-    __syncthreads();
-    if (threadIdx.x == 0) L[j][j] = ljj;
-    for (int i = j + 1 + threadIdx.x; i < nb; i += blockDim.x) L[i][j] /= ljj;
-    __syncthreads();
-    for (int q = threadIdx.x; q < (nb - j - 1) * (nb - j - 1); q += blockDim.x) {
-      const int i = j + 1 + q / (nb - j - 1), c = j + 1 + q % (nb - j - 1);
-      if (c <= i) L[i][c] -= L[i][j] * L[c][j];
-    }
-    __syncthreads();
-  }
-  if (blockIdx.x == 0) {
-    double* D = Dt + (long long)(k / CNB) * CNB * CNB;
-    for (int q = threadIdx.x; q < CNB * CNB; q += blockDim.x) {
-      const int i = q / CNB, j = q % CNB;
-      D[q] = (j <= i) ? L[i][j] : 0.0;
-    }
-    if (threadIdx.x == 0 && bad) *flag = 1;
-  }
   const int i = k + nb + blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n || i >= k + nb + band) return;
   double x[CNB];
@@ -515,11 +519,10 @@ __global__ void k_chol_step(int n, int k, int band, double* __restrict__ A, doub
 #pragma unroll
   for (int j = 0; j < CNB; ++j) {
     if (j < nb) {
-      double v = x[j];
+      x[j] = x[j] / L[j][j];
 #pragma unroll
-      for (int t = 0; t < CNB; ++t)
-        if (t < j) v -= x[t] * L[j][t];
-      x[j] = v / L[j][j];
+      for (int t = j + 1; t < CNB; ++t)
+        if (t < nb) x[t] -= x[j] * L[t][j];
     }
   }
 #pragma unroll

@@ -754,7 +754,7 @@ int topo_ctx_create(int nelx, int nely, int nelz, int n_levels, int mode, int fi
     for (int l = 0; l < n_levels; ++l) {
       Level& Lv = c->L[l];
       const long long nd = Lv.g.ndof;
-      Lv.mask = c->alloc<uint8_t>(nd);
+      Lv.mask = c->alloc<uint8_t>(nd + 16);  // the tensor-core K.u reads aligned 4-byte mask words
       Lv.x = c->valloc(nd);
       Lv.r = c->valloc(nd);
       Lv.d = c->valloc(nd);

@@ -33,7 +33,6 @@ namespace topo {
 
 namespace tc {
 
-constexpr int PX = 16, PY = 16;       // elements per patch in x and y
 constexpr int OWN = 15;               // owned nodes per patch per direction
 constexpr int ZB = 4;                 // element layers per tensor-memory block
 constexpr int RX = 16;                // node slots per row (x), 8 bytes each
@@ -42,8 +41,6 @@ constexpr int NPL = ZB + 1;           // node planes per block
 constexpr int ROW_B = RX * 8;         // 128 bytes
 constexpr int PLANE_B = RX * RY * 8;  // 2176 bytes
 constexpr int COPY_B = NPL * PLANE_B; // 10880 bytes
-constexpr int NLEV = ZB + 1;          // output node levels staged per block
-constexpr int OUT_FLOATS = OWN * OWN * NLEV * 3;
 constexpr int al16(int x) { return (x + 15) & ~15; }
 static_assert(PLANE_B % 16 == 0, "descriptor alignment");
 
@@ -139,38 +136,71 @@ __device__ __forceinline__ float ldu(const TU* p) {
 // Persistent warp-specialised pipeline. One CTA per SM walks a contiguous
 // range of (column, z-layer) items, column = one 16x16-element patch, in
 // blocks of ZB layers; four roles overlap successive blocks:
-//   load   (warps 8-11): node planes -> BF16 records in a 3-stage ring
-//   mma    (warp 12, one thread): 4 tcgen05.mma per layer into one of two
+//   load   (warps 12-14): node planes -> BF16 records, 2-stage ring
+//   mma    (warp 15, one thread): 4 tcgen05.mma per layer into one of two
 //          256-column TMEM buffers, commit -> tfull[tb] and empty[s]
-//   reduce (warps 0-3 = TMEM lanes 0-127): TMEM -> E scaling -> nodal sums
-//          (x pair in registers, y by shuffles, z by a carried share) ->
-//          staged outputs (two buffers)
-//   store  (warps 4-7): the epilogue (Store / Residual / RUpd / ChebR) on the
-//          owned nodes of the block, z-contiguous
+//   reduce (warps 0-3 = TMEM lanes 0-127): TMEM -> E scaling -> sums over
+//          the x pair (registers) and the y pair (shuffles inside a warp;
+//          the row below a warp's first row goes to a small boundary
+//          table) -> partial nodal values per layer and z side (dz = 0, 1)
+//          into a double-buffered partial table. No barriers inside.
+//   store  (warps 4-11): per owned DoF, level L = dz0 part of layer L +
+//          dz1 part of layer L-1 (carried in registers across blocks), then
+//          the epilogue (Store / Residual / RUpd / ChebR). The epilogue's
+//          inputs (mask word, r, dinv, x, u or b) for the NEXT block are
+//          prefetched into shared memory with cp.async while this block is
+//          processed; each thread prefetches exactly the slots it consumes.
 // Every wait is an mbarrier poll with an iteration limit; a timeout raises
 // the device error flag and a CTA-wide abort so the other roles stop too.
-constexpr int NSTAGE = 3;
+constexpr int NSTAGE = 2;
 constexpr int STAGE_B = 2 * COPY_B;
-constexpr int OUT_B = al16(OUT_FLOATS * 4);
-constexpr int NT2 = 416;
-constexpr int W_STORE = 4, W_LOAD = 8, W_MMA = 12;
+// 16 warps: each SM sub-partition holds 4, so 128 registers a thread fit
+// the 16K registers of a sub-partition.
+constexpr int NT2 = 512;
+constexpr int W_STORE = 4, W_LOAD = 12, W_MMA = 15;
+constexpr int NL_THREADS = 32 * (W_MMA - W_LOAD);
+constexpr int NS_THREADS = 256;
+constexpr int SLOT_COL = 12;                          // ZB levels x 3 components
+constexpr int SLOTS = 2816;                           // >= 225 * 12, multiple of 256
+constexpr int SLOTS_PER_THREAD = SLOTS / NS_THREADS;  // 11
+constexpr int P_MAIN = ZB * 2 * 3 * OWN * OWN;        // [l][dz][c][yr-1][xr-1]
+constexpr int P_BND = ZB * 2 * 3 * 3 * OWN;           // [l][dz][c][w][xr-1], node rows 4, 8, 12
+constexpr int P_BUF_B = (P_MAIN + P_BND) * 4;
+constexpr int N_IN = 5;                               // mask word + up to four vectors
+constexpr int IN_BUF_B = N_IN * SLOTS * 4;
 constexpr int P_B = 0;
 constexpr int P_ST = 2048;
-constexpr int P_OUT = al16(P_ST + NSTAGE * STAGE_B);
-constexpr int P_XCH = al16(P_OUT + 2 * OUT_B);
-constexpr int P_BAR = al16(P_XCH + 4 * 8 * 12 * 4);
-constexpr int NBAR = 2 * NSTAGE + 8;  // full[3] empty[3] tfull[2] tempty[2] ofull[2] oempty[2]
+constexpr int P_P = al16(P_ST + NSTAGE * STAGE_B);
+constexpr int P_IN = al16(P_P + 2 * P_BUF_B);
+constexpr int P_BAR = al16(P_IN + 2 * IN_BUF_B);
+constexpr int NBAR = 2 * NSTAGE + 8;  // full[2] empty[2] tfull[2] tempty[2] ofull[2] oempty[2]
 constexpr int P_TMEM = al16(P_BAR + NBAR * 8);
 constexpr int P_ABORT = P_TMEM + 4;
-constexpr int SMEM2_BYTES = P_ABORT + 4 + 1024;
-constexpr int SMEM2_REQUEST = 120 * 1024;  // one CTA per SM: it owns all 512 TMEM columns
+constexpr int SMEM2_REQUEST = P_ABORT + 4 + 1024;  // one CTA per SM: it owns all 512 TMEM columns
 constexpr uint32_t TMEM2_COLS = 512;
-static_assert(SMEM2_BYTES <= SMEM2_REQUEST, "shared memory budget");
+static_assert(SMEM2_REQUEST <= 232448, "shared memory budget");
+static_assert(SLOTS >= OWN * OWN * SLOT_COL && SLOTS % NS_THREADS == 0, "slot table");
 static_assert(P_ST % 16 == 0 && STAGE_B % 16 == 0 && COPY_B % 16 == 0, "descriptor alignment");
 static_assert(P_BAR % 8 == 0, "barrier alignment");
 
+__device__ __forceinline__ int pidx(int l, int dz, int c, int yr1, int xr1) {
+  return (((l * 2 + dz) * 3 + c) * OWN + yr1) * OWN + xr1;
+}
+__device__ __forceinline__ int bidx(int l, int dz, int c, int w, int xr1) {
+  return P_MAIN + (((l * 2 + dz) * 3 + c) * 3 + w) * OWN + xr1;
+}
+
 __device__ __forceinline__ void mbar_arrive(uint32_t bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ void cp_async4(uint32_t dst, const void* src, uint32_t src_size) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(dst), "l"(src), "r"(src_size) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
 // Bounded wait that also gives up when another role has aborted.
@@ -184,8 +214,8 @@ __device__ __forceinline__ bool wait_bar(uint32_t bar, uint32_t parity, volatile
   return false;
 }
 
-// AND of a predicate over the 128 reduce threads (named barrier 1): their
-// decision to stop must be uniform because they meet at that barrier.
+// AND of a predicate over the 128 reduce threads (named barrier 1), so that
+// they stop together.
 __device__ __forceinline__ bool all_reduce_threads(bool pred) {
   uint32_t r;
   asm volatile(
@@ -201,7 +231,8 @@ __device__ __forceinline__ bool all_reduce_threads(bool pred) {
 
 // The block sequence of one CTA: layer items [lo, hi) in column-major order
 // (item = column * nz + z); per column a segment [z0, z1) processed from the
-// seed layer max(0, z0 - 1) in blocks of ZB layers.
+// seed layer max(0, z0 - 1) in blocks of ZB layers. Output levels of a
+// block: [max(zb, z0), zb + nb), plus level nz after the last layer.
 struct BlockSeq {
   int nz, lo, hi, c, c_hi, zb, z0, z1;
   __device__ void seg() {
@@ -219,6 +250,7 @@ struct BlockSeq {
   __device__ bool valid() const { return lo < hi && c <= c_hi; }
   __device__ int nb() const { return min(ZB, z1 - zb); }
   __device__ bool first() const { return zb == max(0, z0 - 1); }
+  __device__ int zlo() const { return max(zb, z0); }
   __device__ void next() {
     zb += ZB;
     if (zb >= z1) {
@@ -227,6 +259,35 @@ struct BlockSeq {
     }
   }
 };
+
+// Epilogue on prefetched inputs (same arithmetic as epilogue_store).
+template <Epi EPI>
+__device__ __forceinline__ void epi_apply(const EpiDev<float>& e, long long i, bool fr, float acc, float a0, float a1,
+                                          float a2, float a3) {
+  if constexpr (EPI == Epi::Store) {
+    e.y[i] = fr ? acc : 0.f;
+  } else if constexpr (EPI == Epi::Residual) {
+    e.y[i] = fr ? a0 - acc : 0.f;
+  } else if constexpr (EPI == Epi::RUpd) {
+    e.r[i] = fr ? a0 - e.s * acc : 0.f;
+  } else if constexpr (EPI == Epi::ChebR) {
+    if (fr) {
+      const float rv = a0 - e.s * acc;
+      e.r[i] = rv;
+      const float dn = e.c1 * a3 + e.c2 * (a1 * rv);
+      e.d_out[i] = dn;
+      e.x[i] = a2 + e.ax * dn;
+    } else {
+      e.r[i] = 0.f;
+      e.d_out[i] = 0.f;
+    }
+  }
+}
+
+template <Epi EPI>
+__host__ __device__ constexpr int n_inputs() {
+  return EPI == Epi::ChebR ? 4 : (EPI == Epi::Store ? 0 : 1);
+}
 
 // q(dx,dy,dz) = dx + 2 dy + 4 dz indexes the 8 corners; output column q*4+c.
 template <typename TU, Epi EPI>
@@ -248,14 +309,14 @@ k_level0_tc(Grid g, const TU* __restrict__ u, const float* __restrict__ E, const
     reinterpret_cast<uint4*>(sm + P_B)[i] = reinterpret_cast<const uint4*>(Bglob)[i];
   if (tid == 0) {
     for (int s = 0; s < NSTAGE; ++s) {
-      mbar_init(bar_full + 8 * s, 128);
+      mbar_init(bar_full + 8 * s, NL_THREADS);
       mbar_init(bar_empty + 8 * s, 1);
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(bar_tfull + 8 * b, 1);
       mbar_init(bar_tempty + 8 * b, 128);
       mbar_init(bar_ofull + 8 * b, 128);
-      mbar_init(bar_oempty + 8 * b, 128);
+      mbar_init(bar_oempty + 8 * b, NS_THREADS);
     }
     *abort_flag = 0;
   }
@@ -279,27 +340,38 @@ k_level0_tc(Grid g, const TU* __restrict__ u, const float* __restrict__ E, const
 
   if (warp >= W_LOAD && warp < W_MMA) {
     // ------------------------------------------------------------ load
+    // All node loads of a block are issued before the wait for the stage, so
+    // they overlap with the previous block's MMA and with each other.
     const int pt = tid - 32 * W_LOAD;
+    constexpr int NCOL = 17 * 17, CPT = (NCOL + NL_THREADS - 1) / NL_THREADS;
     for (int k = 0; q.valid(); ++k, q.next()) {
       const int s = k % NSTAGE;
-      if (!wait_bar(bar_empty + 8 * s, ((k / NSTAGE) & 1) ^ 1, abort_flag, errflag)) break;
       const int x0 = -1 + OWN * (q.c / ncoly), y0 = -1 + OWN * (q.c % ncoly);
       const int zb = q.zb, nb = q.nb();
-      unsigned char* A0 = sm + P_ST + s * STAGE_B;
-      unsigned char* A1 = A0 + COPY_B;
-      for (int cidx = pt; cidx < 17 * 17; cidx += 128) {
+      float v[CPT][ZB + 1][3];
+#pragma unroll
+      for (int t = 0; t < CPT; ++t) {
+        const int cidx = pt + NL_THREADS * t;
         const int xs = cidx % 17, ys = cidx / 17;
         const int gx = x0 + xs, gyy = y0 + ys;
-        const bool in = gx >= 0 && gx < g.NX && gyy >= 0 && gyy < g.NY;
+        const bool in = cidx < NCOL && gx >= 0 && gx < g.NX && gyy >= 0 && gyy < g.NY;
         const long long n0 = ((long long)gx * g.NY + gyy) * g.NZ + zb;
-        float v[ZB + 1][3];
 #pragma unroll
         for (int pz = 0; pz <= ZB; ++pz)
 #pragma unroll
-          for (int c = 0; c < 3; ++c) v[pz][c] = (in && pz <= nb) ? ldu(u + 3 * (n0 + pz) + c) : 0.f;
+          for (int c = 0; c < 3; ++c) v[t][pz][c] = (in && pz <= nb) ? ldu(u + 3 * (n0 + pz) + c) : 0.f;
+      }
+      if (!wait_bar(bar_empty + 8 * s, ((k / NSTAGE) & 1) ^ 1, abort_flag, errflag)) break;
+      unsigned char* A0 = sm + P_ST + s * STAGE_B;
+      unsigned char* A1 = A0 + COPY_B;
+#pragma unroll
+      for (int t = 0; t < CPT; ++t) {
+        const int cidx = pt + NL_THREADS * t;
+        if (cidx >= NCOL) break;
+        const int xs = cidx % 17, ys = cidx / 17;
 #pragma unroll
         for (int pz = 0; pz <= ZB; ++pz) {
-          const uint2 rec = pack_node(v[pz][0], v[pz][1], v[pz][2]);
+          const uint2 rec = pack_node(v[t][pz][0], v[t][pz][1], v[t][pz][2]);
           if (xs < RX) *reinterpret_cast<uint2*>(A0 + pz * PLANE_B + ys * ROW_B + xs * 8) = rec;
           if (xs >= 1) *reinterpret_cast<uint2*>(A1 + pz * PLANE_B + ys * ROW_B + (xs - 1) * 8) = rec;
         }
@@ -341,18 +413,10 @@ k_level0_tc(Grid g, const TU* __restrict__ u, const float* __restrict__ E, const
   } else if (warp < W_STORE) {
     // ---------------------------------------------------------- reduce
     const int m = tid, gy = m >> 3, r = m & 7;
-    float* xch = reinterpret_cast<float*>(sm + P_XCH);
-    float carry[2][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
     for (int k = 0; q.valid(); ++k, q.next()) {
       const int tb = k & 1, ob = k & 1;
       const int x0 = -1 + OWN * (q.c / ncoly), y0 = -1 + OWN * (q.c % ncoly);
-      const int zb = q.zb, nb = q.nb(), z0 = q.z0, z1 = q.z1;
-      if (q.first()) {
-#pragma unroll
-        for (int nd = 0; nd < 2; ++nd)
-#pragma unroll
-          for (int c = 0; c < 3; ++c) carry[nd][c] = 0.f;
-      }
+      const int zb = q.zb, nb = q.nb();
       // moduli of this thread's two elements, fetched before the wait
       float EA[ZB], EB[ZB];
       const int ex = x0 + 2 * r, ey = y0 + gy;
@@ -367,11 +431,10 @@ k_level0_tc(Grid g, const TU* __restrict__ u, const float* __restrict__ E, const
       ok = ok && wait_bar(bar_oempty + 8 * ob, ((k >> 1) & 1) ^ 1, abort_flag, errflag);
       if (!all_reduce_threads(ok)) break;
       tc_fence_after();
-      float* outs = reinterpret_cast<float*>(sm + P_OUT + ob * OUT_B);
+      float* P = reinterpret_cast<float*>(sm + P_P + ob * P_BUF_B);
 #pragma unroll
       for (int l = 0; l < ZB; ++l) {
         if (l >= nb) break;
-        const int z = zb + l;
         float OA[32], OB[32];
         const uint32_t tl = tbase + ((uint32_t)(warp * 32) << 16) + tb * 256 + l * 64;
         tmem_ld32(tl, OA);
@@ -394,103 +457,158 @@ k_level0_tc(Grid g, const TU* __restrict__ u, const float* __restrict__ E, const
               S[0][dy][dz][c] = a_hi + b_lo;
               S[1][dy][dz][c] = b_hi + next_a_lo;
             }
-        if (lane >= 24) {
-          float* xo = xch + (warp * 8 + (lane - 24)) * 12;
+        // node row gy: dy=0 share of element row gy + dy=1 share of row gy-1
 #pragma unroll
-          for (int nd = 0; nd < 2; ++nd)
-#pragma unroll
-            for (int dz = 0; dz < 2; ++dz)
-#pragma unroll
-              for (int c = 0; c < 3; ++c) xo[(nd * 2 + dz) * 3 + c] = S[nd][1][dz][c];
-        }
-        asm volatile("bar.sync 1, 128;" ::: "memory");
-        float U[2][2][3];
-#pragma unroll
-        for (int nd = 0; nd < 2; ++nd)
+        for (int nd = 0; nd < 2; ++nd) {
+          const int xr = 2 * r + 1 + nd;
 #pragma unroll
           for (int dz = 0; dz < 2; ++dz)
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
-              float prev = __shfl_up_sync(0xffffffffu, S[nd][1][dz][c], 8);
-              if (lane < 8) prev = (warp > 0) ? xch[((warp - 1) * 8 + lane) * 12 + (nd * 2 + dz) * 3 + c] : 0.f;
-              U[nd][dz][c] = S[nd][0][dz][c] + prev;
+              const float up = __shfl_up_sync(0xffffffffu, S[nd][1][dz][c], 8);
+              const float v = S[nd][0][dz][c] + (lane >= 8 ? up : 0.f);
+              if (xr <= OWN && gy >= 1) P[pidx(l, dz, c, gy - 1, xr - 1)] = v;
+              if (xr <= OWN && lane >= 24 && warp < 3) P[bidx(l, dz, c, warp, xr - 1)] = S[nd][1][dz][c];
             }
-        const int lev = z - zb;
-#pragma unroll
-        for (int nd = 0; nd < 2; ++nd) {
-          const int xr = 2 * r + 1 + nd;
-          const bool own = xr <= OWN && gy >= 1;
-#pragma unroll
-          for (int c = 0; c < 3; ++c) {
-            const float v = U[nd][0][c] + carry[nd][c];
-            carry[nd][c] = U[nd][1][c];
-            if (own && z >= z0) outs[(((gy - 1) * OWN + (xr - 1)) * NLEV + lev) * 3 + c] = v;
-          }
         }
-        asm volatile("bar.sync 1, 128;" ::: "memory");  // xch reuse
       }
       tc_fence_before();
       mbar_arrive(bar_tempty + 8 * tb);
-      if ((zb + nb == z1) && (z1 == g.nz)) {
-#pragma unroll
-        for (int nd = 0; nd < 2; ++nd) {
-          const int xr = 2 * r + 1 + nd;
-          if (xr <= OWN && gy >= 1)
-#pragma unroll
-            for (int c = 0; c < 3; ++c) outs[(((gy - 1) * OWN + (xr - 1)) * NLEV + nb) * 3 + c] = carry[nd][c];
-        }
-      }
       mbar_arrive(bar_ofull + 8 * ob);
     }
   } else {
     // ----------------------------------------------------------- store
+    // Slot j of this thread is the fixed (column, position) pair
+    // sidx = stid + 256 j -> column sidx / 12, position sidx % 12 = lv*3 + c,
+    // so its geometry is computed once: K[j] = the DoF offset from the
+    // block's first owned DoF, tag[j] = packed (x, y, lv, c, boundary row).
     const int stid = tid - 32 * W_STORE;
+    constexpr int NIN = n_inputs<EPI>();
+    constexpr bool U_IN = (EPI == Epi::ChebR) && sizeof(TU) == 4;
+    const float* in_src[4] = {nullptr, nullptr, nullptr, nullptr};
+    if constexpr (EPI == Epi::Residual) in_src[0] = ep.b;
+    if constexpr (EPI == Epi::RUpd) in_src[0] = ep.r;
+    if constexpr (EPI == Epi::ChebR) {
+      in_src[0] = ep.r;
+      in_src[1] = ep.dinv;
+      in_src[2] = ep.x;
+      in_src[3] = reinterpret_cast<const float*>(u);
+    }
+    const long long sx = 3LL * g.NZ * g.NY, sy = 3LL * g.NZ;
+    int K[SLOTS_PER_THREAD];  // < 16 * 3 * NZ * NY + 12, well inside int range for any mesh that fits
+    uint32_t tag[SLOTS_PER_THREAD];  // xr1 | yr1 << 4 | lv << 8 | c << 10 | bnd << 12, or ~0 when unused
+#pragma unroll
+    for (int j = 0; j < SLOTS_PER_THREAD; ++j) {
+      const int sidx = stid + NS_THREADS * j;
+      const int col = sidx / SLOT_COL, rem = sidx - SLOT_COL * col;
+      const int xr1 = col % OWN, yr1 = col / OWN;
+      const int lv = rem / 3, c = rem - 3 * lv;
+      K[j] = (int)((xr1 + 1) * sx + (yr1 + 1) * sy + rem);
+      tag[j] = col < OWN * OWN ? (uint32_t)(xr1 | (yr1 << 4) | (lv << 8) | (c << 10) | ((((yr1 + 1) & 3) == 0) << 12))
+                               : 0xffffffffu;
+    }
+    struct BlkGeo {
+      long long C;   // DoF index of (x0, y0, zlo), component 0
+      int xlim, ylim, per_col, sd;
+    };
+    auto geo = [&](const BlockSeq& b) {
+      BlkGeo r;
+      const int x0 = -1 + OWN * (b.c / ncoly), y0 = -1 + OWN * (b.c % ncoly);
+      const int zlo = b.zlo();
+      r.C = x0 * sx + y0 * sy + 3LL * zlo;
+      r.xlim = g.NX - 1 - x0;
+      r.ylim = g.NY - 1 - y0;
+      r.per_col = (b.zb + b.nb() - zlo) * 3;
+      r.sd = zlo - b.zb;
+      return r;
+    };
+    auto slot_ok = [&](uint32_t t, const BlkGeo& gb, int rem_pos) {
+      return t != 0xffffffffu && rem_pos < gb.per_col && (int)(t & 15) + 1 <= gb.xlim &&
+             (int)((t >> 4) & 15) + 1 <= gb.ylim;
+    };
+    auto prefetch = [&](const BlockSeq& b, int buf) {
+      const BlkGeo gb = geo(b);
+      const uint32_t base = smem_u32(sm + P_IN + buf * IN_BUF_B);
+#pragma unroll
+      for (int j = 0; j < SLOTS_PER_THREAD; ++j) {
+        const int sidx = stid + NS_THREADS * j;
+        const uint32_t t = tag[j];
+        const int rem = (int)((t >> 8) & 3) * 3 + (int)((t >> 10) & 3);
+        const bool val = slot_ok(t, gb, rem);
+        const long long i = val ? gb.C + K[j] : 0;
+        cp_async4(base + 4 * sidx, mask + (i & ~3LL), val ? 4u : 0u);
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+          if (a < NIN && (a < 3 || U_IN)) cp_async4(base + 4 * ((a + 1) * SLOTS + sidx), in_src[a] + i, val ? 4u : 0u);
+      }
+      cp_async_commit();
+    };
+    BlockSeq pf = q;
+    if (pf.valid()) prefetch(pf, 0);
+    float carry[SLOTS_PER_THREAD];
+#pragma unroll
+    for (int j = 0; j < SLOTS_PER_THREAD; ++j) carry[j] = 0.f;
     for (int k = 0; q.valid(); ++k, q.next()) {
       const int ob = k & 1;
+      pf.next();
+      if (pf.valid()) prefetch(pf, (k + 1) & 1);
+      else cp_async_commit();
+      cp_async_wait<1>();
       if (!wait_bar(bar_ofull + 8 * ob, (k >> 1) & 1, abort_flag, errflag)) break;
-      const float* outs = reinterpret_cast<const float*>(sm + P_OUT + ob * OUT_B);
-      const int x0 = -1 + OWN * (q.c / ncoly), y0 = -1 + OWN * (q.c % ncoly);
-      const int zb = q.zb, nb = q.nb();
-      const bool last_level = (zb + nb == q.z1) && (q.z1 == g.nz);
-      const int zlo = max(zb, q.z0);
-      const int nlev_out = (zb + nb) - zlo + (last_level ? 1 : 0);
-      if (nlev_out > 0) {
-        const int per_node = nlev_out * 3;
-        const int total = OWN * OWN * per_node;
-        for (int base = stid; base < total; base += 4 * 128) {
-          long long ii[4];
-          float acc[4], ui[4];
-          bool val[4], fr[4];
+      const float* P = reinterpret_cast<const float*>(sm + P_P + ob * P_BUF_B);
+      const float* inb = reinterpret_cast<const float*>(sm + P_IN + ob * IN_BUF_B);
+      const BlkGeo gb = geo(q);
+      const int nb = q.nb();
+      if (q.first()) {
 #pragma unroll
-          for (int j = 0; j < 4; ++j) {
-            const int idx = base + 128 * j;
-            val[j] = false;
-            ii[j] = 0;
-            acc[j] = 0.f;
-            if (idx < total) {
-              const int on = idx / per_node, rem = idx % per_node;
-              const int lv = rem / 3, c = rem % 3;
-              const int xr = on % OWN + 1, yr = on / OWN + 1;
-              const int gx = x0 + xr, gyy = y0 + yr, gz = zlo + lv;
-              if (gx < g.NX && gyy < g.NY && gz < g.NZ) {
-                val[j] = true;
-                ii[j] = 3 * (((long long)gx * g.NY + gyy) * g.NZ + gz) + c;
-                acc[j] = outs[(on * NLEV + (gz - zb)) * 3 + c];
-              }
+        for (int j = 0; j < SLOTS_PER_THREAD; ++j) carry[j] = 0.f;
+      }
+      const bool last_level = (q.zb + nb == q.z1) && (q.z1 == g.nz);
+#pragma unroll
+      for (int j = 0; j < SLOTS_PER_THREAD; ++j) {
+        const int sidx = stid + NS_THREADS * j;
+        const uint32_t t = tag[j];
+        if (t == 0xffffffffu) continue;
+        const int xr1 = t & 15, yr1 = (t >> 4) & 15, lv = (t >> 8) & 3, c = (t >> 10) & 3;
+        if (xr1 + 1 > gb.xlim || yr1 + 1 > gb.ylim) continue;
+        const int off = yr1 * OWN + xr1;
+        const int boff = P_MAIN + (((yr1 + 1) >> 2) - 1) * OWN + xr1;
+        const bool bnd = (t >> 12) & 1;
+        auto part = [&](int l, int dz) {
+          const int lc = (l * 2 + dz) * 3 + c;
+          float v = P[lc * (OWN * OWN) + off];
+          if (bnd) v += P[lc * (3 * OWN) + boff];
+          return v;
+        };
+        const int rem = lv * 3 + c;
+        if (rem < gb.per_col) {
+          const int l = lv + gb.sd;
+          const float acc = part(l, 0) + (l >= 1 ? part(l - 1, 1) : carry[j]);
+          const long long i = gb.C + K[j];
+          const uint32_t mw = __float_as_uint(inb[sidx]);
+          const bool fr = ((mw >> (8 * (int)(i & 3))) & 0xffu) != 0;
+          const float a3 = U_IN ? inb[4 * SLOTS + sidx] : (EPI == Epi::ChebR ? ldu(u + i) : 0.f);
+          epi_apply<EPI>(ep, i, fr, acc, inb[SLOTS + sidx], inb[2 * SLOTS + sidx], inb[3 * SLOTS + sidx], a3);
+        }
+        if (lv == 0) {
+          // carry for level zb + nb: dz1 share of the last layer
+          carry[j] = part(nb - 1, 1);
+          if (last_level) {
+            const long long i = gb.C + K[j] + 3LL * (g.nz - q.zlo());
+            float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
+            if constexpr (NIN >= 1) a0 = in_src[0][i];
+            if constexpr (NIN >= 4) {
+              a1 = in_src[1][i];
+              a2 = in_src[2][i];
+              a3 = ldu(u + i);
             }
+            epi_apply<EPI>(ep, i, mask[i] != 0, carry[j], a0, a1, a2, a3);
           }
-#pragma unroll
-          for (int j = 0; j < 4; ++j) {
-            fr[j] = val[j] ? mask[ii[j]] != 0 : false;
-            ui[j] = (EPI == Epi::ChebR && val[j]) ? ldu(u + ii[j]) : 0.f;
-          }
-#pragma unroll
-          for (int j = 0; j < 4; ++j)
-            if (val[j]) epilogue_store<float, EPI>(ep, ii[j], fr[j], acc[j], ui[j]);
         }
       }
       mbar_arrive(bar_oempty + 8 * ob);
     }
+    cp_async_wait<0>();
   }
   tc_fence_before();
   __syncthreads();
@@ -561,7 +679,8 @@ static void launch_tc(const Grid& g, const void* u, const void* E, const uint8_t
 }
 
 // BF16-input K.u on the tensor cores. u_bf16: u stored as BF16 (else FP32,
-// rounded when staged). Supports the Store, Residual, RUpd and ChebR epilogues.
+// rounded when staged). `mask` must stay readable 16 bytes past the last DoF
+// (the store role prefetches aligned 4-byte mask words). Supports the Store, Residual, RUpd and ChebR epilogues.
 void level0_apply_tc(bool u_bf16, const Grid& g, const void* u, const void* E, const uint8_t* mask, void* y, Epi epi,
                      const EpiArgs& ea, cudaStream_t s) {
   if (!g_tcB) throw std::runtime_error("tensor-core operator not prepared");
