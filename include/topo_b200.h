@@ -127,11 +127,33 @@ int topo_pcg(topo_ctx* ctx, const void* b, void* x, double tol, int maxiter, int
 int topo_fgmres(topo_ctx* ctx, const void* b, void* x, double tol, int maxiter, int restart,
                 int* out_iters, double* out_relres, void* stream);
 
+/* Block PCG for nrhs load cases (1..8) on the current hierarchy: B and X are
+ * nrhs full-length FP64 vectors stored one after another (X holds the
+ * initial guesses and receives the solutions). One multi-vector FP64 K.u per
+ * iteration (moduli staged once for all columns), the GMG V-cycle on every
+ * column, alpha/beta from nrhs x nrhs Gram matrices; columns leave the block
+ * once ||r_j|| <= tol ||mask b_j||. out_relres receives nrhs values.
+ * Returns 0 (all converged), 1 (maxiter reached) or < 0. The reference solves
+ * one load case per PCG (_cupy_pcg, src/gpu_fem/solver_v2.py:552-624); this
+ * replaces nrhs of those calls. */
+int topo_block_pcg(topo_ctx* ctx, const double* B, double* X, int nrhs, double tol, int maxiter,
+                   int* out_iters, double* out_relres, void* stream);
+
 /* Element-energy sensitivity dc_e = -penal (E0-Emin) rho_e^(penal-1) u_e^T KE u_e
  * with u in u_dtype (TOPO_F64 or TOPO_F32), FP64 arithmetic.
  * Replaces src/gpu_fem/solver_v4.py:246-251. */
 int topo_sensitivity(topo_ctx* ctx, const void* u, int u_dtype, const double* rho, double penal,
                      double E0, double Emin, double* dc, void* stream);
+
+/* Adjoint sensitivity of a linear functional J = L^T u with K(rho) u = F:
+ * with lam from K lam = L (a second GMG-PCG solve on the same hierarchy),
+ * dJ/drho_e = -penal (E0-Emin) rho_e^(penal-1) lam_e^T KE u_e, written to dc.
+ * lam = u gives the compliance sensitivity. u and lam share `dtype`
+ * (TOPO_F64 or TOPO_F32). The reference differentiates only compliance
+ * (src/gpu_fem/solver_v4.py:244-251); this is the non-self-adjoint form of
+ * the same element contraction. */
+int topo_sensitivity_adjoint(topo_ctx* ctx, const void* u, const void* lam, int dtype, const double* rho,
+                             double penal, double E0, double Emin, double* dc, void* stream);
 
 /* FP64 dot product sum_i a_i b_i (a,b in dtype TOPO_F64 or TOPO_F32); the
  * result is written to *out_host (synchronises the stream). Used for the

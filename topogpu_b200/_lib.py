@@ -36,7 +36,9 @@ SIGNATURES = {
     "topo_gmg_apply": (_i, [_vp, _vp, _vp, _vp]),
     "topo_pcg": (_i, [_vp, _vp, _vp, _d, _i, C.POINTER(_i), C.POINTER(_d), _vp]),
     "topo_fgmres": (_i, [_vp, _vp, _vp, _d, _i, _i, C.POINTER(_i), C.POINTER(_d), _vp]),
+    "topo_block_pcg": (_i, [_vp, _vp, _vp, _i, _d, _i, C.POINTER(_i), C.POINTER(_d), _vp]),
     "topo_sensitivity": (_i, [_vp, _vp, _i, _vp, _d, _d, _d, _vp, _vp]),
+    "topo_sensitivity_adjoint": (_i, [_vp, _vp, _vp, _i, _vp, _d, _d, _d, _vp, _vp]),
     "topo_dot": (_i, [_vp, _i, _vp, _vp, _ll, C.POINTER(_d), _vp]),
     "topo_filter": (_i, [_vp, _d, _vp, _vp, _i, _vp]),
     "topo_oc": (_i, [_vp, _vp, _vp, _d, _d, _d, _vp, C.POINTER(_i), _vp]),

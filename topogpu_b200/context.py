@@ -147,6 +147,20 @@ class TopoContext:
                                              int(restart), C.byref(it), C.byref(rr), _stream()), "fgmres")
         return it.value, rr.value, rc == 0
 
+    def block_pcg(self, B, X, tol=1e-5, maxiter=800):
+        """Block PCG over the rows of B (nrhs x ndof, float64); X (same shape)
+        holds initial guesses and receives the solutions. Returns
+        (iterations, [relres per column], all_converged)."""
+        if B.dim() != 2 or B.shape != X.shape or B.shape[1] != self.ndof:
+            raise ValueError("block_pcg: B and X must be (nrhs, ndof)")
+        nrhs = int(B.shape[0])
+        it = C.c_int(0)
+        rr = (C.c_double * nrhs)()
+        rc = self._chk(self._lib.topo_block_pcg(self._h, _ptr(B, torch.float64, nrhs * self.ndof, "B"),
+                                                _ptr(X, torch.float64, nrhs * self.ndof, "X"), nrhs, float(tol),
+                                                int(maxiter), C.byref(it), rr, _stream()), "block_pcg")
+        return it.value, list(rr), rc == 0
+
     # -- design ------------------------------------------------------------
     def sensitivity(self, u, rho, penal=3.0, E0=1.0, Emin=1e-9, out=None):
         dt = _DT.get(u.dtype)
@@ -156,6 +170,19 @@ class TopoContext:
         self._chk(self._lib.topo_sensitivity(self._h, _ptr(u, None, self.ndof, "u"), dt,
                                              _ptr(rho, torch.float64, self.n_elem, "rho"), penal, E0, Emin,
                                              _ptr(out, torch.float64, self.n_elem, "dc"), _stream()), "sensitivity")
+        return out
+
+    def sensitivity_adjoint(self, u, lam, rho, penal=3.0, E0=1.0, Emin=1e-9, out=None):
+        """dJ/drho for J = L^T u given the adjoint lam (K lam = L)."""
+        dt = _DT.get(u.dtype)
+        if dt not in (_lib.F64, _lib.F32) or lam.dtype != u.dtype:
+            raise TypeError("u and lam must both be float64 or both float32")
+        out = torch.empty(self.n_elem, dtype=torch.float64, device=u.device) if out is None else out
+        self._chk(self._lib.topo_sensitivity_adjoint(self._h, _ptr(u, None, self.ndof, "u"),
+                                                     _ptr(lam, None, self.ndof, "lam"), dt,
+                                                     _ptr(rho, torch.float64, self.n_elem, "rho"), penal, E0, Emin,
+                                                     _ptr(out, torch.float64, self.n_elem, "dc"), _stream()),
+                  "sensitivity_adjoint")
         return out
 
     def dot(self, a, b) -> float:

@@ -166,6 +166,12 @@ struct topo_ctx {
   // FGMRES basis (allocated on demand)
   std::vector<void*> fg_V, fg_Z;
   KrylovState* st = nullptr;
+  // block PCG workspace (FP64 columns R, Z, P, Q, Pn; allocated per block width)
+  int blk_nv = 0;
+  double* blk = nullptr;
+  double* blk_part = nullptr;
+  double* blk_G = nullptr;
+  double* blk_Gh = nullptr;  // pinned host copy
   KrylovState* h_st = nullptr;  // pinned host mirror
   RedWork red{};
   double* dtmp = nullptr;       // 64 device doubles
@@ -620,6 +626,184 @@ int do_pcg(topo_ctx* c, const double* b, double* x, double tol, int maxiter, int
 // and Givens rotations (multigrid_v4.py:325-443). The Hessenberg factor is
 // tiny and lives on the host; vectors and dots stay on the device; the
 // iterate is FP64 and every restart starts from the FP64 true residual.
+// ------------------------------------------------------------ block PCG
+// Block preconditioned CG (O'Leary) for nv load cases on one density field,
+// with the GMG V-cycle on every column and one multi-vector FP64 K.u per
+// iteration; alpha = (P^T Q)^-1 (Z^T R), beta = (Z_old^T R_old)^-1 (Z^T R)
+// on the host (nv x nv, Cholesky). A column whose relative residual reaches
+// tol leaves the block (its X stays). Returns 0 when every column converged.
+static bool small_chol_solve(int k, const double* A, const double* B, double* X) {
+  // A (k x k SPD, stride 8), B (k x k, stride 8) -> X = A^-1 B
+  double L[8][8] = {};
+  for (int j = 0; j < k; ++j) {
+    double d = A[j * 8 + j];
+    for (int t = 0; t < j; ++t) d -= L[j][t] * L[j][t];
+    if (!(d > 0.0) || !std::isfinite(d)) return false;
+    L[j][j] = std::sqrt(d);
+    for (int i = j + 1; i < k; ++i) {
+      double v = A[i * 8 + j];
+      for (int t = 0; t < j; ++t) v -= L[i][t] * L[j][t];
+      L[i][j] = v / L[j][j];
+    }
+  }
+  for (int col = 0; col < k; ++col) {
+    double y[8];
+    for (int i = 0; i < k; ++i) {
+      double v = B[i * 8 + col];
+      for (int t = 0; t < i; ++t) v -= L[i][t] * y[t];
+      y[i] = v / L[i][i];
+    }
+    for (int i = k - 1; i >= 0; --i) {
+      double v = y[i];
+      for (int t = i + 1; t < k; ++t) v -= L[t][i] * X[t * 8 + col];
+      X[i * 8 + col] = v / L[i][i];
+    }
+  }
+  return true;
+}
+
+int do_block_pcg(topo_ctx* c, const double* B, double* X, int nv, double tol, int maxiter, int* out_iters,
+                 double* out_relres, cudaStream_t s) {
+  Level& L0 = c->L[0];
+  const long long n = L0.g.ndof;
+  if (c->blk_nv != nv) {
+    c->blk = c->alloc<double>(5LL * nv * n);
+    if (!c->blk_part) {
+      c->blk_part = c->alloc<double>((long long)block_gram_partials());
+      c->blk_G = c->alloc<double>(64);
+      TOPO_CUDA_CHECK(cudaMallocHost(&c->blk_Gh, 64 * sizeof(double)));
+    }
+    c->blk_nv = nv;
+  }
+  double *R0 = c->blk, *Z0 = R0 + (long long)nv * n, *P0 = Z0 + (long long)nv * n, *Q0 = P0 + (long long)nv * n,
+         *N0 = Q0 + (long long)nv * n;
+  auto col = [&](double* base, int j) { return base + (long long)j * n; };
+  auto gram = [&](double* const* A, int na, double* const* Bm, int nb, double* Gout) {
+    block_gram(n, (const double* const*)A, na, (const double* const*)Bm, nb, c->blk_part, c->blk_G, s);
+    TOPO_CUDA_CHECK(cudaMemcpyAsync(c->blk_Gh, c->blk_G, 64 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    TOPO_CUDA_CHECK(cudaStreamSynchronize(s));
+    std::memcpy(Gout, c->blk_Gh, 64 * sizeof(double));
+  };
+  auto precond = [&](const double* r, double* z) {
+    if (c->vec64) {
+      vcycle_apply(c, r, z, nullptr, s);
+    } else {
+      vcast(n, r, true, c->kr, false, s);
+      vcycle_apply(c, c->kr, c->kz, nullptr, s);
+      vcast(n, c->kz, false, z, true, s);
+    }
+  };
+  std::vector<int> act;
+  double* Xc[8];
+  double* Rc[8];
+  double* Zc[8];
+  double* Pc[8];
+  double* Qc[8];
+  double* Nc[8];
+  const double* Bc[8];
+  for (int j = 0; j < nv; ++j) {
+    Xc[j] = X + (long long)j * n;
+    Bc[j] = B + (long long)j * n;
+    Rc[j] = col(R0, j);
+    Zc[j] = col(Z0, j);
+    Pc[j] = col(P0, j);
+    Qc[j] = col(Q0, j);
+    Nc[j] = col(N0, j);
+  }
+  // masked right-hand sides and their norms (Z used as scratch)
+  for (int j = 0; j < nv; ++j) {
+    TOPO_CUDA_CHECK(cudaMemcpyAsync(Zc[j], Bc[j], sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+    vmask(true, n, Zc[j], L0.mask, s);
+  }
+  double G[64], H[64], A8[64], Bm8[64];
+  gram(Zc, nv, Zc, nv, G);
+  double bnorm[8];
+  for (int j = 0; j < nv; ++j) bnorm[j] = std::sqrt(std::max(G[j * 8 + j], 0.0));
+  // R = mask(B) - A X
+  level0_apply_block(L0.g, (const double* const*)Xc, c->E64, L0.mask, Qc, nv, s);
+  {
+    double I8[64] = {};
+    for (int j = 0; j < 8; ++j) I8[j * 8 + j] = 1.0;
+    block_combine(n, (const double* const*)Qc, nv, (const double* const*)Zc, Rc, nv, I8, -1.0, s);
+  }
+  gram(Rc, nv, Rc, nv, G);
+  for (int j = 0; j < nv; ++j) {
+    const double rel = bnorm[j] > 0 ? std::sqrt(std::max(G[j * 8 + j], 0.0)) / bnorm[j] : 0.0;
+    out_relres[j] = rel;
+    if (rel > tol) act.push_back(j);
+  }
+  int it = 0;
+  auto pick = [&](double* const* all, double** out) {
+    for (size_t a = 0; a < act.size(); ++a) out[a] = all[act[a]];
+  };
+  double *aR[8], *aZ[8], *aP[8], *aQ[8], *aN[8], *aX[8];
+  double rz[64];
+  if (!act.empty()) {
+    pick(Rc, aR);
+    pick(Zc, aZ);
+    pick(Pc, aP);
+    const int k = (int)act.size();
+    for (int a = 0; a < k; ++a) {
+      precond(aR[a], aZ[a]);
+      TOPO_CUDA_CHECK(cudaMemcpyAsync(aP[a], aZ[a], sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+    }
+    gram(aZ, k, aR, k, rz);
+    it = 1;
+  }
+  while (!act.empty() && it <= maxiter) {
+    const int k = (int)act.size();
+    pick(Rc, aR);
+    pick(Zc, aZ);
+    pick(Pc, aP);
+    pick(Qc, aQ);
+    pick(Nc, aN);
+    pick(Xc, aX);
+    level0_apply_block(L0.g, (const double* const*)aP, c->E64, L0.mask, aQ, k, s);
+    gram(aP, k, aQ, k, G);  // P^T Q
+    if (!small_chol_solve(k, G, rz, A8)) throw std::runtime_error("block PCG: P^T K P lost definiteness");
+    block_combine(n, (const double* const*)aP, k, (const double* const*)aX, aX, k, A8, 1.0, s);
+    block_combine(n, (const double* const*)aQ, k, (const double* const*)aR, aR, k, A8, -1.0, s);
+    gram(aR, k, aR, k, G);
+    std::vector<int> keep;
+    for (int a = 0; a < k; ++a) {
+      const int j = act[a];
+      const double rel = std::sqrt(std::max(G[a * 8 + a], 0.0)) / bnorm[j];
+      out_relres[j] = rel;
+      if (rel > tol) keep.push_back(a);
+    }
+    if (keep.empty()) {
+      act.clear();
+      break;
+    }
+    if (it == maxiter) break;
+    // deflate: restrict the old Z^T R to the surviving columns
+    const int k2 = (int)keep.size();
+    double rz_old[64] = {};
+    for (int a = 0; a < k2; ++a)
+      for (int b2 = 0; b2 < k2; ++b2) rz_old[a * 8 + b2] = rz[keep[a] * 8 + keep[b2]];
+    std::vector<int> act2;
+    for (int a : keep) act2.push_back(act[a]);
+    act = act2;
+    pick(Rc, aR);
+    pick(Zc, aZ);
+    pick(Pc, aP);
+    pick(Nc, aN);
+    for (int a = 0; a < k2; ++a) precond(aR[a], aZ[a]);
+    gram(aZ, k2, aR, k2, H);  // Z^T R
+    // P's surviving columns
+    double* Pk[8];
+    for (int a = 0; a < k2; ++a) Pk[a] = aP[a];
+    if (!small_chol_solve(k2, rz_old, H, Bm8)) throw std::runtime_error("block PCG: Z^T R lost definiteness");
+    block_combine(n, (const double* const*)Pk, k2, (const double* const*)aZ, aN, k2, Bm8, 1.0, s);
+    // the new directions live in N: swap the column roles P <-> N
+    for (int a = 0; a < k2; ++a) std::swap(Pc[act[a]], Nc[act[a]]);
+    std::memcpy(rz, H, sizeof(rz));
+    ++it;
+  }
+  *out_iters = it;
+  return act.empty() ? 0 : 1;
+}
+
 int do_fgmres(topo_ctx* c, const double* b, double* x, double tol, int maxiter, int restart, int* out_iters,
               double* out_relres, cudaStream_t s) {
   Level& L0 = c->L[0];
@@ -728,6 +912,7 @@ int topo_ctx_create(int nelx, int nely, int nelz, int n_levels, int mode, int fi
     c->cheb_lower = cheb_lower;
     c->dense_max = dense_max;
     set_ke(KE_host);
+    set_ke_block(KE_host);
     std::vector<double> Q(8 * 576);
     host_galerkin_q(KE_host, Q.data());
     set_galerkin_q(Q.data());
@@ -814,6 +999,7 @@ int topo_ctx_destroy(topo_ctx* c) {
   if (c->cs) cudaStreamSynchronize(c->cs);
   for (void* p : c->allocs) cudaFree(p);
   if (c->h_st) cudaFreeHost(c->h_st);
+  if (c->blk_Gh) cudaFreeHost(c->blk_Gh);
   if (c->ev_in) cudaEventDestroy(c->ev_in);
   if (c->ev_out) cudaEventDestroy(c->ev_out);
   for (auto& e : c->ev_ph)
@@ -1008,13 +1194,40 @@ int topo_fgmres(topo_ctx* c, const void* b, void* x, double tol, int maxiter, in
   }
 }
 
+int topo_block_pcg(topo_ctx* c, const double* B, double* X, int nrhs, double tol, int maxiter, int* out_iters,
+                   double* out_relres, void* stream) {
+  try {
+    if (!c || !B || !X || !out_iters || !out_relres) throw std::invalid_argument("topo_block_pcg: null pointer");
+    if (!c->setup_done) throw std::runtime_error("topo_block_pcg: call topo_gmg_setup first");
+    if (nrhs < 1 || nrhs > 8) throw std::invalid_argument("topo_block_pcg: nrhs must be 1..8");
+    if (maxiter < 1) throw std::invalid_argument("topo_block_pcg: maxiter must be >= 1");
+    StreamGuard sg(c, stream);
+    return do_block_pcg(c, B, X, nrhs, tol, maxiter, out_iters, out_relres, c->cs);
+  } catch (const std::exception& e) {
+    return fail(c, e);
+  }
+}
+
 int topo_sensitivity(topo_ctx* c, const void* u, int u_dtype, const double* rho, double penal, double E0,
                      double Emin, double* dc, void* stream) {
   try {
     if (!c || !u || !rho || !dc) throw std::invalid_argument("topo_sensitivity: null pointer");
     if (u_dtype != TOPO_F64 && u_dtype != TOPO_F32) throw std::invalid_argument("topo_sensitivity: bad dtype");
     StreamGuard sg(c, stream);
-    sensitivity(c->L[0].g, u, u_dtype == TOPO_F32, rho, penal, E0, Emin, dc, c->cs);
+    sensitivity(c->L[0].g, u, nullptr, u_dtype == TOPO_F32, rho, penal, E0, Emin, dc, c->cs);
+    return 0;
+  } catch (const std::exception& e) {
+    return fail(c, e);
+  }
+}
+
+int topo_sensitivity_adjoint(topo_ctx* c, const void* u, const void* lam, int dtype, const double* rho,
+                             double penal, double E0, double Emin, double* dc, void* stream) {
+  try {
+    if (!c || !u || !lam || !rho || !dc) throw std::invalid_argument("topo_sensitivity_adjoint: null pointer");
+    if (dtype != TOPO_F64 && dtype != TOPO_F32) throw std::invalid_argument("topo_sensitivity_adjoint: bad dtype");
+    StreamGuard sg(c, stream);
+    sensitivity(c->L[0].g, u, lam, dtype == TOPO_F32, rho, penal, E0, Emin, dc, c->cs);
     return 0;
   } catch (const std::exception& e) {
     return fail(c, e);

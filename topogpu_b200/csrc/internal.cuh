@@ -216,8 +216,9 @@ void level0_apply_tc(bool u_bf16, const Grid& g, const void* u, const void* E, c
 int tc_error_flag(cudaStream_t s);
 void modulus(long long n, const double* rho, double penal, double E0, double Emin, double* E,
              float* E32, cudaStream_t s);
-void sensitivity(const Grid& g, const void* u, bool u_f32, const double* rho, double penal, double E0,
-                 double Emin, double* dc, cudaStream_t s);
+// dc_e = -penal (E0-Emin) rho_e^(penal-1) v_e^T KE u_e (v = u when null)
+void sensitivity(const Grid& g, const void* u, const void* v, bool u_f32, const double* rho, double penal,
+                 double E0, double Emin, double* dc, cudaStream_t s);
 
 // coarse levels (coarse.cu): 27-point block stencils S[k*9 + c*3 + d][node]
 void level1_assemble(const Grid& fine, const Grid& coarse, const double* E_f, const uint8_t* mask_c,
@@ -249,6 +250,18 @@ void dense_apply_prepare(int n);
 // x = scatter(W^T W gather(rhs)); y is n FP64 scratch
 void dense_apply(bool vec64, int n, long long ldc, const double* C64, const float* C32, const int* free_list,
                  const void* rhs, double* y, void* x, const KrylovState* st, cudaStream_t s);
+
+// block PCG kernels (blockops.cu): FP64 column blocks as pointer lists
+void set_ke_block(const double* KE_host);
+void level0_apply_block(const Grid& g, const double* const* U, const double* E, const uint8_t* mask,
+                        double* const* Y, int nv, cudaStream_t s);
+size_t block_gram_partials();
+// G[i*8+j] = A_i . B_j (device, 64 doubles); part: block_gram_partials() doubles
+void block_gram(long long n, const double* const* A, int na, const double* const* B, int nb, double* part,
+                double* G, cudaStream_t s);
+// Out_j = C_j + sign * sum_i In_i M[i*8+j] (C may be null, Out may alias C)
+void block_combine(long long n, const double* const* In, int ni, const double* const* Cc, double* const* Out, int no,
+                   const double* M, double sign, cudaStream_t s);
 
 // vectors and reductions (vec.cu)
 void vfill(bool f64, long long n, void* x, double v, cudaStream_t s);

@@ -303,12 +303,13 @@ void modulus(long long n, const double* rho, double penal, double E0, double Emi
 // dc_e = -p (E0-Emin) rho^(p-1) u_e^T KE u_e, FP64 arithmetic
 // (src/gpu_fem/solver_v4.py:246-251).
 template <typename TU>
-__global__ void k_sensitivity(Grid g, const TU* __restrict__ u, const double* __restrict__ rho, double penal,
-                              double E0, double Emin, double* __restrict__ dc) {
+__global__ void k_sensitivity(Grid g, const TU* __restrict__ u, const TU* __restrict__ v,
+                              const double* __restrict__ rho, double penal, double E0, double Emin,
+                              double* __restrict__ dc) {
   const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (e >= g.nelem) return;
   const int ez = e % g.nz, ey = (e / g.nz) % g.ny, ex = e / ((long long)g.nz * g.ny);
-  double ue[24];
+  double ue[24], ve[24];
 #pragma unroll
   for (int m = 0; m < 8; ++m) {
     const int bx = (m == 1 || m == 2 || m == 5 || m == 6);
@@ -316,29 +317,52 @@ __global__ void k_sensitivity(Grid g, const TU* __restrict__ u, const double* __
     const int bz = (m >= 4);
     const long long n = ((long long)(ex + bx) * g.NY + (ey + by)) * g.NZ + (ez + bz);
 #pragma unroll
-    for (int c = 0; c < 3; ++c) ue[3 * m + c] = (double)u[3 * n + c];
+    for (int c = 0; c < 3; ++c) {
+      ue[3 * m + c] = (double)u[3 * n + c];
+      ve[3 * m + c] = (v != nullptr) ? (double)v[3 * n + c] : ue[3 * m + c];
+    }
   }
+  // KE annihilates rigid translations, so the element means are removed
+  // first: v_e^T KE u_e is unchanged and the contraction no longer cancels
+  // the (large) translation part of the displacement in rounding.
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    double mu = 0.0, mv = 0.0;
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+      mu += ue[3 * m + c];
+      mv += ve[3 * m + c];
+    }
+    mu *= 0.125;
+    mv *= 0.125;
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+      ue[3 * m + c] -= mu;
+      ve[3 * m + c] -= mv;
+    }
+  }
+  // ce = v_e^T KE u_e (KE symmetric), v = u for compliance
   double ce = 0.0;
 #pragma unroll
   for (int i = 0; i < 24; ++i) {
     double t = 0.0;
 #pragma unroll
     for (int j = 0; j < 24; ++j) t += ue[j] * cKE64[j * 24 + i];
-    ce += t * ue[i];
+    ce += t * ve[i];
   }
   const double r = rho[e];
   const double rp = (penal == 3.0) ? r * r : pow(r, penal - 1.0);
   dc[e] = -penal * (E0 - Emin) * rp * ce;
 }
 
-void sensitivity(const Grid& g, const void* u, bool u_f32, const double* rho, double penal, double E0,
-                 double Emin, double* dc, cudaStream_t s) {
+void sensitivity(const Grid& g, const void* u, const void* v, bool u_f32, const double* rho, double penal,
+                 double E0, double Emin, double* dc, cudaStream_t s) {
   const int bs = 128;
   const unsigned nb = (unsigned)((g.nelem + bs - 1) / bs);
   if (u_f32)
-    k_sensitivity<float><<<nb, bs, 0, s>>>(g, (const float*)u, rho, penal, E0, Emin, dc);
+    k_sensitivity<float><<<nb, bs, 0, s>>>(g, (const float*)u, (const float*)v, rho, penal, E0, Emin, dc);
   else
-    k_sensitivity<double><<<nb, bs, 0, s>>>(g, (const double*)u, rho, penal, E0, Emin, dc);
+    k_sensitivity<double><<<nb, bs, 0, s>>>(g, (const double*)u, (const double*)v, rho, penal, E0, Emin, dc);
   TOPO_LAUNCH_CHECK();
 }
 

@@ -100,6 +100,24 @@ class StateSolver:
                                 "outer_solver": self.outer, "cg_iters": it}
         return float(compliance), dc
 
+    def solve_block(self, rho, loads, penal: float = 3.0):
+        """Several load cases on one density field with block PCG.
+
+        loads: (nrhs, ndof) float64 (fixed DoFs ignored). Returns
+        (compliances F_j . u_j as a list, U as an (nrhs, ndof) tensor). The
+        hierarchy is set up once for all load cases."""
+        dev = self.device
+        rho = torch.as_tensor(rho, dtype=torch.float64, device=dev).contiguous()
+        B = torch.as_tensor(loads, dtype=torch.float64, device=dev).contiguous()
+        self.ctx.modulus(rho, penal, self.E0, self.Emin, out=self.E)
+        self.ctx.gmg_setup(self.E)
+        U = torch.zeros_like(B)
+        it, rr, ok = self.ctx.block_pcg(B, U, self.tol, self.maxiter)
+        self.last_cg_iters, self.last_relres, self.last_converged = it, max(rr), ok
+        self.last_outer_solver = "block_pcg"
+        Bm = B * self.free_mask
+        return [float(torch.dot(Bm[j], U[j])) for j in range(B.shape[0])], U
+
     def displacement(self) -> torch.Tensor:
         """Last displacement (full length, fixed DoFs zero) in FP64."""
         return self.u
