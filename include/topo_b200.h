@@ -136,6 +136,11 @@ int topo_fgmres(topo_ctx* ctx, const void* b, void* x, double tol, int maxiter, 
  * Returns 0 (all converged), 1 (maxiter reached) or < 0. The reference solves
  * one load case per PCG (_cupy_pcg, src/gpu_fem/solver_v2.py:552-624); this
  * replaces nrhs of those calls. */
+/* BF16 level-0 operator on the tensor cores (on != 0, the default) or on the
+ * CUDA cores (same BF16 inputs and FP32 accumulation, another summation
+ * order); a tuning switch with no reference counterpart. */
+int topo_set_tc(topo_ctx* ctx, int on);
+
 int topo_block_pcg(topo_ctx* ctx, const double* B, double* X, int nrhs, double tol, int maxiter,
                    int* out_iters, double* out_relres, void* stream);
 

@@ -147,6 +147,10 @@ class TopoContext:
                                              int(restart), C.byref(it), C.byref(rr), _stream()), "fgmres")
         return it.value, rr.value, rc == 0
 
+    def set_tensor_cores(self, on: bool):
+        """BF16 level-0 K.u on tcgen05 (True) or on the CUDA cores (False)."""
+        self._chk(self._lib.topo_set_tc(self._h, int(bool(on))), "set_tc")
+
     def block_pcg(self, B, X, tol=1e-5, maxiter=800):
         """Block PCG over the rows of B (nrhs x ndof, float64); X (same shape)
         holds initial guesses and receives the solutions. Returns

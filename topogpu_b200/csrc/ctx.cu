@@ -67,10 +67,23 @@ __global__ void k_dinv_from_diag(long long n, const double* __restrict__ diag, c
   }
 }
 
+// Start vector of the power iterations on the free DoFs: all ones (the
+// reference's choice), or, for the Chebyshev-iteration smoother, a fixed
+// pseudo-random vector (splitmix64 of the index, values of both signs) whose
+// high-frequency content makes 10-20 steps reach the top of the spectrum.
+__device__ __forceinline__ double hashed_unit(unsigned long long i) {
+  unsigned long long z = i + 0x9E3779B97F4A7C15ULL;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+  z ^= z >> 31;
+  const double u = (double)(z >> 11) * (1.0 / 9007199254740992.0);  // [0, 1)
+  return (u < 0.5 ? -1.0 : 1.0) * (0.5 + u);
+}
+
 template <typename T>
-__global__ void k_mask_to(long long n, const uint8_t* __restrict__ m, T* __restrict__ v) {
+__global__ void k_mask_to(long long n, const uint8_t* __restrict__ m, T* __restrict__ v, int random) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-    v[i] = m[i] ? (T)1 : (T)0;
+    v[i] = m[i] ? (random ? (T)hashed_unit((unsigned long long)i) : (T)1) : (T)0;
 }
 
 template <typename T>
@@ -166,6 +179,11 @@ struct topo_ctx {
   // FGMRES basis (allocated on demand)
   std::vector<void*> fg_V, fg_Z;
   KrylovState* st = nullptr;
+  // PCG iteration graph, kept across solves while its key (everything the
+  // capture bakes in: Chebyshev bounds, options, buffer addresses) is unchanged
+  cudaGraphExec_t pcg_exec = nullptr;
+  long long pcg_exec_kernels = 0;
+  std::vector<double> pcg_key;
   // block PCG workspace (FP64 columns R, Z, P, Q, Pn; allocated per block width)
   int blk_nv = 0;
   double* blk = nullptr;
@@ -330,8 +348,9 @@ double lambda_fine(topo_ctx* c, cudaStream_t s) {
   void* Kv = L0.r;
   void* Av = L0.d2;
   double* d = c->dtmp;
-  if (f64) k_mask_to<double><<<gblocks(n), 256, 0, s>>>(n, L0.mask, (double*)v);
-  else k_mask_to<float><<<gblocks(n), 256, 0, s>>>(n, L0.mask, (float*)v);
+  const int rnd = c->cheb_form == 1;
+  if (f64) k_mask_to<double><<<gblocks(n), 256, 0, s>>>(n, L0.mask, (double*)v, rnd);
+  else k_mask_to<float><<<gblocks(n), 256, 0, s>>>(n, L0.mask, (float*)v, rnd);
   TOPO_LAUNCH_CHECK();
   auto dotdiv = [&](const void* a, const void* b) {
     if (f64) k_dot_div<double><<<kRedBlocks, kRedThreads, 0, s>>>(n, (const double*)a, (const double*)b, (const double*)L0.dinv, d, c->red);
@@ -369,7 +388,7 @@ double lambda_coarse(topo_ctx* c, int l, double* dinv64, cudaStream_t s) {
   double* V = c->C.scrA;
   double* KV = c->C.scrB;
   double* AV = c->C.scrC;
-  k_mask_to<double><<<gblocks(n), 256, 0, s>>>(n, Lv.mask, V);
+  k_mask_to<double><<<gblocks(n), 256, 0, s>>>(n, Lv.mask, V, c->cheb_form == 1);
   TOPO_LAUNCH_CHECK();
   double* d = c->dtmp;
   double nrm0 = std::sqrt(dot_host(true, n, V, V, c->red, d, s));
@@ -517,6 +536,18 @@ void pcg_iteration(topo_ctx* c, cudaStream_t s) {
   pcg_p_update(c->vec64, n, c->kz, c->kp, c->st, false, s);
 }
 
+std::vector<double> pcg_graph_key(const topo_ctx* c) {
+  std::vector<double> k = {(double)c->cheb_form, c->lam_safety, c->cheb_lower, (double)c->use_tc,
+                           (double)c->fine_degree, (double)c->coarse_degree,
+                           (double)reinterpret_cast<uintptr_t>(c->C.work), (double)reinterpret_cast<uintptr_t>(c->C.X32),
+                           (double)reinterpret_cast<uintptr_t>(c->C.y), (double)c->C.n, (double)c->C.ldc};
+  for (const Level& Lv : c->L) {
+    k.push_back(std::isnan(Lv.lam) ? -1.0 : Lv.lam);  // NaN (no estimate) would never compare equal
+    k.push_back((double)Lv.degree);
+  }
+  return k;
+}
+
 void read_state(topo_ctx* c, cudaStream_t s) {
   TOPO_CUDA_CHECK(cudaMemcpyAsync(c->h_st, c->st, sizeof(KrylovState), cudaMemcpyDeviceToHost, s));
   TOPO_CUDA_CHECK(cudaStreamSynchronize(s));
@@ -557,9 +588,15 @@ int do_pcg(topo_ctx* c, const double* b, double* x, double tol, int maxiter, int
   double rr = true_residual(c, s);
   int iters = 0;
   bool converged = rr <= tol2;  // up-front check (solver_v2.py:594-596)
-  // one PCG iteration recorded once as a CUDA graph on the context stream
-  cudaGraphExec_t exec = nullptr;
-  long long graph_kernels = 0;
+  // one PCG iteration recorded as a CUDA graph on the context stream, reused
+  // by later solves while nothing it captured has changed
+  const std::vector<double> key = pcg_graph_key(c);
+  if (c->pcg_exec && key != c->pcg_key) {
+    cudaGraphExecDestroy(c->pcg_exec);
+    c->pcg_exec = nullptr;
+  }
+  cudaGraphExec_t exec = c->pcg_exec;
+  long long graph_kernels = c->pcg_exec_kernels;
   int refreshes = 0;
   while (!converged && iters < maxiter && refreshes < 8) {
     k_set_state<<<1, 1, 0, s>>>(c->st, bb, tol2);
@@ -578,6 +615,9 @@ int do_pcg(topo_ctx* c, const double* b, double* x, double tol, int maxiter, int
       count_launches(-graph_kernels);
       TOPO_CUDA_CHECK(cudaGraphInstantiate(&exec, graph, 0));
       TOPO_CUDA_CHECK(cudaGraphDestroy(graph));
+      c->pcg_exec = exec;
+      c->pcg_exec_kernels = graph_kernels;
+      c->pcg_key = key;
     }
     const int base = iters;  // V-cycles applied before this run of iterations
     int launched = 0;
@@ -612,7 +652,6 @@ int do_pcg(topo_ctx* c, const double* b, double* x, double tol, int maxiter, int
     }
     ++refreshes;
   }
-  if (exec) cudaGraphExecDestroy(exec);
   rr = true_residual(c, s);
   TOPO_CUDA_CHECK(cudaMemcpyAsync(x, c->kx64, vb, cudaMemcpyDeviceToDevice, s));
   if (out_iters) *out_iters = iters;
@@ -1000,6 +1039,7 @@ int topo_ctx_destroy(topo_ctx* c) {
   for (void* p : c->allocs) cudaFree(p);
   if (c->h_st) cudaFreeHost(c->h_st);
   if (c->blk_Gh) cudaFreeHost(c->blk_Gh);
+  if (c->pcg_exec) cudaGraphExecDestroy(c->pcg_exec);
   if (c->ev_in) cudaEventDestroy(c->ev_in);
   if (c->ev_out) cudaEventDestroy(c->ev_out);
   for (auto& e : c->ev_ph)
@@ -1189,6 +1229,16 @@ int topo_fgmres(topo_ctx* c, const void* b, void* x, double tol, int maxiter, in
     if (maxiter < 1 || restart < 1) throw std::invalid_argument("topo_fgmres: maxiter and restart must be >= 1");
     StreamGuard sg(c, stream);
     return do_fgmres(c, (const double*)b, (double*)x, tol, maxiter, restart, out_iters, out_relres, c->cs);
+  } catch (const std::exception& e) {
+    return fail(c, e);
+  }
+}
+
+int topo_set_tc(topo_ctx* c, int on) {
+  try {
+    if (!c) throw std::invalid_argument("topo_set_tc: null context");
+    c->use_tc = on != 0;
+    return 0;
   } catch (const std::exception& e) {
     return fail(c, e);
   }

@@ -118,6 +118,10 @@ class StateSolver:
         Bm = B * self.free_mask
         return [float(torch.dot(Bm[j], U[j])) for j in range(B.shape[0])], U
 
+    def reset_warm_start(self):
+        """Make the next solve start from u = 0."""
+        self._have_prev = False
+
     def displacement(self) -> torch.Tensor:
         """Last displacement (full length, fixed DoFs zero) in FP64."""
         return self.u
