@@ -139,6 +139,14 @@ int topo_fgmres(topo_ctx* ctx, const void* b, void* x, double tol, int maxiter, 
 /* BF16 level-0 operator on the tensor cores (on != 0, the default) or on the
  * CUDA cores (same BF16 inputs and FP32 accumulation, another summation
  * order); a tuning switch with no reference counterpart. */
+/* Lagged coarsest factor (on != 0): from the second topo_gmg_setup on, the
+ * V-cycle applies the coarsest factor of the previous setup while the factor
+ * of the current operator is built on a background stream (it replaces the
+ * old one at the next setup). The preconditioner stays symmetric positive
+ * definite; Krylov solves still converge to their tolerance. Off by default;
+ * the reference refactorises synchronously (multigrid_v4.py:774-811). */
+int topo_set_coarse_lag(topo_ctx* ctx, int on);
+
 int topo_set_tc(topo_ctx* ctx, int on);
 
 int topo_block_pcg(topo_ctx* ctx, const double* B, double* X, int nrhs, double tol, int maxiter,
@@ -218,8 +226,10 @@ int topo_field_stats(topo_ctx* ctx, const double* x, long long n, double* out_ho
 int topo_gmg_info(topo_ctx* ctx, long long* n_free, double* lambda_max, int* coarse_kind);
 /* Device time (ms) of the phases of the last topo_gmg_setup: ms[0] fine
  * diagonal and lambda_max check, ms[1] coarse stencils (level-1 Galerkin,
- * R.A.P, Jacobi, lambda, conversions), ms[2] coarsest dense assembly,
- * ms[3] banded Cholesky, ms[4] W = L^-1. Diagnostic of GalerkinMatFreeGMG.setup
+ * R.A.P, Jacobi, lambda, conversions), ms[2] copy of the coarsest stencil,
+ * ms[3] coarsest factorisation (assembly, banded Cholesky and W = L^-1, one
+ * graph; 0 when it runs in the background under topo_set_coarse_lag),
+ * ms[4] pivot check and eps*I retry. Diagnostic of GalerkinMatFreeGMG.setup
  * (src/gpu_fem/multigrid_v4.py:657-811), which the reference times only as a
  * whole in SolverV4.last_timing (solver_v4.py:231-267). */
 int topo_setup_phases(topo_ctx* ctx, double* ms);

@@ -321,3 +321,28 @@ def test_simpsolver_evidence_bundle(cuda_dev, tmp_path):
                       "wall_s", "outer_solver"}
     assert abs(h["rho_mean"] - 0.3) < 1e-6
     assert len(b.rows) == 4
+
+
+@pytest.mark.gpu
+def test_lagged_coarse_factor_same_solutions(cuda_dev):
+    """With the one-setup-lagged coarsest factor (built in the background) the
+    solves converge to the same compliances as with the synchronous factor."""
+    from topogpu_b200.bc import cantilever_edge_load
+    from topogpu_b200.state import StateSolver
+
+    nel = (48, 24, 24)
+    mask, F = cantilever_edge_load(nel)
+    rng = np.random.default_rng(17)
+    rhos = [torch.tensor(rng.uniform(0.05, 1.0, 48 * 24 * 24), device=DEV) for _ in range(4)]
+    out = {}
+    for lag in (False, True):
+        st = StateSolver(nel, mask, F, n_levels=4, precision="mixed", tol=1e-6, device=DEV)
+        st.ctx.set_coarse_lag(lag)
+        comps = []
+        for r in rhos:
+            c, _ = st.solve(r)
+            assert st.last_converged
+            comps.append(c)
+        out[lag] = np.array(comps)
+        st.close()
+    assert np.max(np.abs(out[True] - out[False]) / np.abs(out[False])) < 1e-5

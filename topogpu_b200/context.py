@@ -147,6 +147,11 @@ class TopoContext:
                                              int(restart), C.byref(it), C.byref(rr), _stream()), "fgmres")
         return it.value, rr.value, rc == 0
 
+    def set_coarse_lag(self, on: bool):
+        """Apply the previous setup's coarsest factor while the new one builds
+        in the background (see topo_set_coarse_lag)."""
+        self._chk(self._lib.topo_set_coarse_lag(self._h, int(bool(on))), "set_coarse_lag")
+
     def set_tensor_cores(self, on: bool):
         """BF16 level-0 K.u on tcgen05 (True) or on the CUDA cores (False)."""
         self._chk(self._lib.topo_set_tc(self._h, int(bool(on))), "set_tc")
@@ -242,7 +247,7 @@ class TopoContext:
         """Device milliseconds of the phases of the last gmg_setup."""
         ms = (C.c_double * 5)()
         self._chk(self._lib.topo_setup_phases(self._h, ms), "setup_phases")
-        return dict(zip(("fine_diag_lambda", "coarse_stencils", "coarsest_assembly", "cholesky", "inverse"),
+        return dict(zip(("fine_diag_lambda", "coarse_stencils", "coarsest_copy", "coarsest_factor", "pivot_check"),
                         list(ms)))
 
     def level_operator(self, level: int) -> torch.Tensor:

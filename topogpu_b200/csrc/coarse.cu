@@ -468,49 +468,63 @@ void dense_assemble(const Grid& g, const double* S, const int* dof_index, int n,
 // read as L afterwards.
 constexpr int CNB = 32;
 
-// One panel step. In every CTA, warp 0 factors the (k,k) block in registers
-// (lane i holds row i; column j is broadcast with shuffles), the same
-// arithmetic in each CTA so all agree; CTA 0 stores it in Dt and raises
-// `flag` on a non-positive or non-finite pivot (the pivot is then taken as
-// 1). Each thread then solves one panel row i in [k+nb, min(n, k+nb+band)),
-// L_ik L_kk^T = A_ik, column by column (the updates of later columns are
-// independent, so they overlap).
-__global__ void k_chol_step(int n, int k, int band, double* __restrict__ A, double* __restrict__ Dt,
-                            int* __restrict__ flag) {
+// One panel step. Every CTA factors the (k,k) block in shared memory (the
+// same arithmetic in each, so all agree): per pivot j one barrier; the
+// trailing entries of the working block take W[i][c] -= W[i][j] W[c][j] / d
+// while column j itself is only read, and its scaled values (sqrt(d) on the
+// diagonal, W[i][j] * rsqrt(d) below) go to a separate output block L. CTA 0
+// stores L in Dt and raises `flag` on a non-positive or non-finite pivot (the
+// pivot is then taken as 1). The block is identity-padded past n, so every
+// loop below runs over the full 32 without predicates. Each thread then
+// solves one panel row i in [k+nb, min(n, k+nb+band)), L_ik L_kk^T = A_ik,
+// column by column with the reciprocal diagonal.
+__global__ void __launch_bounds__(128) k_chol_step(int n, int k, int band, double* __restrict__ A,
+                                                   double* __restrict__ Dt, int* __restrict__ flag) {
+  __shared__ double W[CNB][CNB + 1];
   __shared__ double L[CNB][CNB + 1];
+  __shared__ double invd[CNB];
   const int nb = min(CNB, n - k);
-  if (threadIdx.x < 32) {
-    const int i = threadIdx.x;
-    double a[CNB];
-#pragma unroll
-    for (int c = 0; c < CNB; ++c)
-      a[c] = (i < nb && c < nb && c <= i) ? A[(long long)(k + i) * n + k + c] : (i == c ? 1.0 : 0.0);
-    bool bad = false;
-#pragma unroll
-    for (int j = 0; j < CNB; ++j) {
-      const double d = __shfl_sync(0xffffffffu, a[j], j);
-      const bool ok = d > 0.0 && isfinite(d);
-      bad |= !ok;
-      const double ljj = ok ? sqrt(d) : 1.0;
-      if (i > j) a[j] = a[j] / ljj;
-      else if (i == j) a[j] = ljj;
-#pragma unroll
-      for (int c = j + 1; c < CNB; ++c) {
-        const double lcj = __shfl_sync(0xffffffffu, a[j], c);
-        if (i >= c) a[c] -= a[j] * lcj;
-      }
-    }
-#pragma unroll
-    for (int c = 0; c < CNB; ++c) L[i][c] = (c <= i) ? a[c] : 0.0;
-    if (blockIdx.x == 0) {
-      double* D = Dt + (long long)(k / CNB) * CNB * CNB + i * CNB;
-#pragma unroll
-      for (int c = 0; c < CNB; ++c) D[c] = (c <= i) ? a[c] : 0.0;
-      if (i == 0 && bad) *flag = 1;
-    }
+  const int tid = threadIdx.x;
+  for (int q = tid; q < CNB * CNB; q += blockDim.x) {
+    const int i = q / CNB, j = q % CNB;
+    W[i][j] = (i < nb && j < nb && j <= i) ? A[(long long)(k + i) * n + k + j] : (i == j ? 1.0 : 0.0);
   }
   __syncthreads();
-  const int i = k + nb + blockIdx.x * blockDim.x + threadIdx.x;
+  // thread -> 8 entries of the block: rows r0 + 4m (m < 8), column cc
+  const int cc = tid & 31, r0 = tid >> 5;
+  bool bad = false;
+#pragma unroll 1
+  for (int j = 0; j < CNB; ++j) {
+    const double d = W[j][j];
+    const bool ok = d > 0.0 && isfinite(d);
+    bad |= !ok;
+    const double dd = ok ? d : 1.0;
+    const double inv_d = 1.0 / dd, rs = rsqrt(dd);
+    if (cc == j) {
+#pragma unroll
+      for (int m = 0; m < 8; ++m) {
+        const int i = r0 + 4 * m;
+        if (i == j) L[i][j] = sqrt(dd);
+        else if (i > j) L[i][j] = W[i][j] * rs;
+        else L[i][j] = 0.0;
+      }
+      if (r0 == 0) invd[j] = rs;
+    } else if (cc > j) {
+      const double wcj = W[cc][j] * inv_d;
+#pragma unroll
+      for (int m = 0; m < 8; ++m) {
+        const int i = r0 + 4 * m;
+        if (i >= cc) W[i][cc] -= W[i][j] * wcj;
+      }
+    }
+    __syncthreads();
+  }
+  if (blockIdx.x == 0) {
+    double* D = Dt + (long long)(k / CNB) * CNB * CNB;
+    for (int q = tid; q < CNB * CNB; q += blockDim.x) D[q] = (q % CNB <= q / CNB) ? L[q / CNB][q % CNB] : 0.0;
+    if (tid == 0 && bad) *flag = 1;
+  }
+  const int i = k + nb + blockIdx.x * blockDim.x + tid;
   if (i >= n || i >= k + nb + band) return;
   double x[CNB];
   double* row = A + (long long)i * n + k;
@@ -518,12 +532,9 @@ __global__ void k_chol_step(int n, int k, int band, double* __restrict__ A, doub
   for (int j = 0; j < CNB; ++j) x[j] = (j < nb) ? row[j] : 0.0;
 #pragma unroll
   for (int j = 0; j < CNB; ++j) {
-    if (j < nb) {
-      x[j] = x[j] / L[j][j];
+    x[j] *= invd[j];
 #pragma unroll
-      for (int t = j + 1; t < CNB; ++t)
-        if (t < nb) x[t] -= x[j] * L[t][j];
-    }
+    for (int t = j + 1; t < CNB; ++t) x[t] -= x[j] * L[t][j];
   }
 #pragma unroll
   for (int j = 0; j < CNB; ++j)
@@ -531,25 +542,42 @@ __global__ void k_chol_step(int n, int k, int band, double* __restrict__ A, doub
 }
 
 // Trailing update A[i][j] -= sum_t L[i][t] L[j][t] over the panel, for
-// k+nb <= j <= i < k+nb+band.
-__global__ void k_chol_update(int n, int k, int band, double* __restrict__ A) {
+// k+nb <= j <= i < k+nb+band and i-j <= band. One CTA per lower-triangular
+// 32x32 tile (blockIdx.x enumerates them row by row), 256 threads, four
+// outputs per thread.
+__global__ void __launch_bounds__(256) k_chol_update(int n, int k, int band, double* __restrict__ A) {
   const int nb = min(CNB, n - k);
   const int base = k + nb;
-  const int i = base + blockIdx.y * 16 + threadIdx.y;
-  const int j = base + blockIdx.x * 16 + threadIdx.x;
-  __shared__ double Li[16][CNB + 1], Lj[16][CNB + 1];
   const int lim = min(n, base + band);
-  for (int t = threadIdx.x; t < nb; t += 16) {
-    const int ii = base + blockIdx.y * 16 + threadIdx.y;
-    const int jj = base + blockIdx.x * 16 + threadIdx.y;
-    Li[threadIdx.y][t] = (ii < lim) ? A[(long long)ii * n + k + t] : 0.0;
-    Lj[threadIdx.y][t] = (jj < lim) ? A[(long long)jj * n + k + t] : 0.0;
+  // tile (ti, tj), tj <= ti, from the linear index
+  int ti = (int)((sqrt(8.0 * blockIdx.x + 1.0) - 1.0) * 0.5);
+  while ((ti + 1) * (ti + 2) / 2 <= (int)blockIdx.x) ++ti;
+  while (ti * (ti + 1) / 2 > (int)blockIdx.x) --ti;
+  const int tj = blockIdx.x - ti * (ti + 1) / 2;
+  const int i0 = base + 32 * ti, j0 = base + 32 * tj;
+  if (i0 - (j0 + 31) > band) return;  // whole tile outside the band
+  __shared__ double Li[32][CNB + 1], Lj[32][CNB + 1];
+  for (int q = threadIdx.x; q < 32 * CNB; q += 256) {
+    const int r = q / CNB, t = q % CNB;
+    Li[r][t] = (i0 + r < lim && t < nb) ? A[(long long)(i0 + r) * n + k + t] : 0.0;
+    Lj[r][t] = (j0 + r < lim && t < nb) ? A[(long long)(j0 + r) * n + k + t] : 0.0;
   }
   __syncthreads();
-  if (i >= lim || j >= lim || j > i || i - j > band) return;
-  double s = 0.0;
-  for (int t = 0; t < nb; ++t) s += Li[threadIdx.y][t] * Lj[threadIdx.x][t];
-  A[(long long)i * n + j] -= s;
+  const int r = threadIdx.x >> 3, c0 = (threadIdx.x & 7) * 4;
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll 8
+  for (int t = 0; t < CNB; ++t) {
+    const double li = Li[r][t];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) acc[q] = fma(li, Lj[c0 + q][t], acc[q]);
+  }
+  const int i = i0 + r;
+  if (i >= lim) return;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int j = j0 + c0 + q;
+    if (j < lim && j <= i && i - j <= band) A[(long long)i * n + j] -= acc[q];
+  }
 }
 
 // Inverse of every factored diagonal block (identity-padded, so the last
@@ -695,7 +723,7 @@ __global__ void __launch_bounds__(TIT, 1) k_tri_inverse(int n, int band, const d
   }
 }
 
-int dense_cholesky(int n, int band, double* A, double* Dt, int* flag, cudaStream_t s) {
+void dense_cholesky_launch(int n, int band, double* A, double* Dt, int* flag, cudaStream_t s) {
   TOPO_CUDA_CHECK(cudaMemsetAsync(flag, 0, sizeof(int), s));
   for (int k = 0; k < n; k += CNB) {
     const int nb = std::min(CNB, n - k);
@@ -703,11 +731,15 @@ int dense_cholesky(int n, int band, double* A, double* Dt, int* flag, cudaStream
     k_chol_step<<<std::max(1, (rows + 127) / 128), 128, 0, s>>>(n, k, band, A, Dt, flag);
     TOPO_LAUNCH_CHECK();
     if (rows > 0) {
-      dim3 blk(16, 16), grd((rows + 15) / 16, (rows + 15) / 16);
-      k_chol_update<<<grd, blk, 0, s>>>(n, k, band, A);
+      const int nt = (rows + 31) / 32;
+      k_chol_update<<<nt * (nt + 1) / 2, 256, 0, s>>>(n, k, band, A);
       TOPO_LAUNCH_CHECK();
     }
   }
+}
+
+int dense_cholesky(int n, int band, double* A, double* Dt, int* flag, cudaStream_t s) {
+  dense_cholesky_launch(n, band, A, Dt, flag, s);
   int h_flag = 0;
   TOPO_CUDA_CHECK(cudaMemcpyAsync(&h_flag, flag, sizeof(int), cudaMemcpyDeviceToHost, s));
   TOPO_CUDA_CHECK(cudaStreamSynchronize(s));
@@ -719,11 +751,6 @@ void dense_inverse_factor(int n, int band, const double* A, const double* Dt, do
   const int nT = (n + CNB - 1) / CNB;
   k_block_tri_inv<<<nT, CNB, 0, s>>>(Dt, Di);
   TOPO_LAUNCH_CHECK();
-  static bool attr = false;
-  if (!attr) {
-    TOPO_CUDA_CHECK(cudaFuncSetAttribute(k_tri_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TRI_SMEM));
-    attr = true;
-  }
   k_tri_inverse<<<nT, TIT, TRI_SMEM, s>>>(n, band, A, Di, W64, ldc, C64, C32);
   TOPO_LAUNCH_CHECK();
 }
@@ -792,6 +819,7 @@ void dense_apply_prepare(int n) {
   TOPO_CUDA_CHECK(cudaFuncSetAttribute(k_coarse_lower<float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, a));
   TOPO_CUDA_CHECK(cudaFuncSetAttribute(k_coarse_upper<double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, a));
   TOPO_CUDA_CHECK(cudaFuncSetAttribute(k_coarse_upper<float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, a));
+  TOPO_CUDA_CHECK(cudaFuncSetAttribute(k_tri_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TRI_SMEM));
 }
 
 void dense_apply(bool vec64, int n, long long ldc, const double* C64, const float* C32, const int* free_list,

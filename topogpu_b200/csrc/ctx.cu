@@ -129,20 +129,33 @@ struct Level {
   int degree = 2;
 };
 
-struct Coarsest {
-  int n = 0;
-  int band = 0;
-  int kind = 0;  // 0 none, 1 dense, 2 regularised dense
-  int* dof_index = nullptr;
-  int* free_list = nullptr;
-  long long ldc = 0;        // row stride of work / X32 (n rounded up to 32)
+// One factorisation of the coarsest operator and the graph that builds it.
+struct FactorSlot {
+  int kind = 0;             // 0 none, 1 dense, 2 regularised dense
+  double* S64c = nullptr;   // copy of the coarsest stencil the factor is built from
   double* A = nullptr;      // assembled matrix, then the band of L
   double* Dt = nullptr;     // factored diagonal blocks of L (32x32 each)
   double* Di = nullptr;     // their inverses
   double* work = nullptr;   // W = L^-1 (FP64); with FP64 vectors also W^T above the diagonal
   float* X32 = nullptr;     // FP32 W / W^T apply matrix (FP32 vectors)
+  int* flag = nullptr;      // non-positive pivot seen
+  cudaGraphExec_t graph = nullptr;  // assembly + Cholesky + W, captured once
+  long long graph_kernels = 0;
+};
+
+struct Coarsest {
+  int n = 0;
+  int band = 0;
+  int* dof_index = nullptr;
+  int* free_list = nullptr;
+  long long ldc = 0;        // row stride of work / X32 (n rounded up to 32)
   double* y = nullptr;      // compact FP64 intermediate of the two-pass apply
-  int* flag = nullptr;
+  FactorSlot cur;           // the factor the V-cycle applies
+  FactorSlot nxt;           // with coarse_lag: the factor being built in the background
+  bool have = false;        // cur holds a factor
+  bool bg_pending = false;  // nxt is being built on bg_stream
+  cudaStream_t bg_stream = nullptr;
+  cudaEvent_t ev_copy = nullptr, bg_done = nullptr;
   double* tmp = nullptr;   // FP64 Jacobi inverse of a coarse level when vectors are FP32
   double* scrA = nullptr;  // FP64 scratch vectors for the coarse power iterations
   double* scrB = nullptr;
@@ -164,6 +177,7 @@ struct topo_ctx {
   double lam_safety = 1.25;   // factor on the power-iteration lambda_max
   int dense_max = 16384;
   bool use_tc = true;         // BF16 level-0 operator on tcgen05 (TOPO_B200_NO_TC=1: CUDA cores)
+  bool coarse_lag = false;    // V-cycle uses the previous setup's coarsest factor; the new one builds in the background
   std::vector<Level> L;
   Coarsest C;
   double* E64 = nullptr;
@@ -303,7 +317,7 @@ void coarsest_solve(topo_ctx* c, const KrylovState* st, cudaStream_t s) {
   else k_gather_zero<float><<<gblocks(n_full), 256, 0, s>>>(n_full, (float*)Lv.x);
   TOPO_LAUNCH_CHECK();
   if (c->C.n == 0) return;
-  dense_apply(c->vec64, c->C.n, c->C.ldc, c->C.work, c->C.X32, c->C.free_list, Lv.b, c->C.y, Lv.x, st, s);
+  dense_apply(c->vec64, c->C.n, c->C.ldc, c->C.cur.work, c->C.cur.X32, c->C.free_list, Lv.b, c->C.y, Lv.x, st, s);
 }
 
 // One V-cycle on level l (multigrid_v4.py:986-1008): input Lv.b, output Lv.x.
@@ -446,6 +460,85 @@ void host_galerkin_q(const double* KE, double* Q) {
   }
 }
 
+// ------------------------------------------------ coarsest factorisation
+void alloc_slot(topo_ctx* c, FactorSlot& f) {
+  const int n = c->C.n;
+  const long long nt = (n + 31) / 32;
+  if (f.graph) {
+    cudaGraphExecDestroy(f.graph);
+    f.graph = nullptr;
+  }
+  f.S64c = c->alloc<double>(243LL * c->L[c->n_levels - 1].g.nnodes);
+  f.A = c->alloc<double>((long long)n * n);
+  f.Dt = c->alloc<double>(nt * 1024);
+  f.Di = c->alloc<double>(nt * 1024);
+  f.work = c->alloc<double>((long long)n * c->C.ldc);
+  f.X32 = c->vec64 ? nullptr : c->alloc<float>((long long)n * c->C.ldc);
+  f.flag = c->alloc<int>(1);
+  f.kind = 0;
+}
+
+// Assembly (from the slot's stencil copy), banded Cholesky and W = L^-1 of
+// one slot, captured once as a graph: ~460 small launches become one.
+void slot_graph(topo_ctx* c, FactorSlot& f, cudaStream_t s) {
+  if (f.graph) return;
+  const Level& Lc = c->L[c->n_levels - 1];
+  const int n = c->C.n;
+  cudaGraph_t g;
+  const long long before = launch_count();
+  TOPO_CUDA_CHECK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+  dense_assemble(Lc.g, f.S64c, c->C.dof_index, n, f.A, s);
+  dense_cholesky_launch(n, c->C.band, f.A, f.Dt, f.flag, s);
+  dense_inverse_factor(n, c->C.band, f.A, f.Dt, f.Di, f.work, c->C.ldc, c->vec64 ? f.work : nullptr,
+                       c->vec64 ? nullptr : f.X32, s);
+  TOPO_CUDA_CHECK(cudaStreamEndCapture(s, &g));
+  f.graph_kernels = launch_count() - before;  // recorded, not launched: counted per replay
+  count_launches(-f.graph_kernels);
+  TOPO_CUDA_CHECK(cudaGraphInstantiate(&f.graph, g, 0));
+  TOPO_CUDA_CHECK(cudaGraphDestroy(g));
+}
+
+void slot_launch(topo_ctx* c, FactorSlot& f, cudaStream_t s) {
+  slot_graph(c, f, s);
+  TOPO_CUDA_CHECK(cudaGraphLaunch(f.graph, s));
+  count_launches(f.graph_kernels);
+}
+
+// After a slot's graph has run: read its pivot flag; on a non-positive pivot
+// rebuild it from the stencil copy with eps*I added (multigrid_v4.py:778-811).
+void slot_finish(topo_ctx* c, FactorSlot& f, cudaStream_t s) {
+  int h = 0;
+  TOPO_CUDA_CHECK(cudaMemcpyAsync(&h, f.flag, sizeof(int), cudaMemcpyDeviceToHost, s));
+  TOPO_CUDA_CHECK(cudaStreamSynchronize(s));
+  if (!h) {
+    f.kind = 1;
+    return;
+  }
+  const Level& Lc = c->L[c->n_levels - 1];
+  const int n = c->C.n;
+  dense_assemble(Lc.g, f.S64c, c->C.dof_index, n, f.A, s);
+  k_diag_sum<<<1, 256, 0, s>>>(n, f.A, c->dtmp);
+  TOPO_LAUNCH_CHECK();
+  double dsum;
+  TOPO_CUDA_CHECK(cudaMemcpyAsync(&dsum, c->dtmp, sizeof(double), cudaMemcpyDeviceToHost, s));
+  TOPO_CUDA_CHECK(cudaStreamSynchronize(s));
+  const double eps = std::max(dsum / n * 1e-8, 1e-14);
+  k_add_diag<<<(n + 255) / 256, 256, 0, s>>>(n, f.A, eps);
+  TOPO_LAUNCH_CHECK();
+  if (dense_cholesky(n, c->C.band, f.A, f.Dt, f.flag, s))
+    throw std::runtime_error("coarsest-level Cholesky failed even after eps*I regularisation");
+  dense_inverse_factor(n, c->C.band, f.A, f.Dt, f.Di, f.work, c->C.ldc, c->vec64 ? f.work : nullptr,
+                       c->vec64 ? nullptr : f.X32, s);
+  f.kind = 2;
+}
+
+void coarse_wait_background(topo_ctx* c) {
+  if (c->C.bg_pending) {
+    TOPO_CUDA_CHECK(cudaEventSynchronize(c->C.bg_done));
+    c->C.bg_pending = false;
+  }
+}
+
 void do_setup(topo_ctx* c, const double* E, cudaStream_t s) {
   Level& L0 = c->L[0];
   const long long ne = L0.g.nelem;
@@ -480,37 +573,40 @@ void do_setup(topo_ctx* c, const double* E, cudaStream_t s) {
     if (Lv.prec == Prec::F32 || Lv.prec == Prec::BF16)
       stencil_convert(243LL * Lv.g.nnodes, Lv.S64, Lv.S32, Lv.prec == Prec::BF16 ? Lv.S16 : nullptr, s);
   }
-  // coarsest: dense FP64 Cholesky with the reference's eps*I retry (multigrid_v4.py:778-811)
-  c->C.kind = 0;
+  // coarsest: dense FP64 Cholesky + W = L^-1, one graph per factor slot, with
+  // the reference's eps*I retry (multigrid_v4.py:778-811)
   TOPO_CUDA_CHECK(cudaEventRecord(c->ev_ph[2], s));
   TOPO_CUDA_CHECK(cudaEventRecord(c->ev_ph[3], s));
   TOPO_CUDA_CHECK(cudaEventRecord(c->ev_ph[4], s));
   if (c->n_levels > 1 && c->C.n > 0) {
-    const int l = c->n_levels - 1;
-    Level& Lc = c->L[l];
-    const int n = c->C.n;
-    dense_assemble(Lc.g, Lc.S64, c->C.dof_index, n, c->C.A, s);
-    TOPO_CUDA_CHECK(cudaEventRecord(c->ev_ph[3], s));
-    int bad = dense_cholesky(n, c->C.band, c->C.A, c->C.Dt, c->C.flag, s);
-    if (bad) {
-      dense_assemble(Lc.g, Lc.S64, c->C.dof_index, n, c->C.A, s);
-      k_diag_sum<<<1, 256, 0, s>>>(n, c->C.A, c->dtmp);
-      TOPO_LAUNCH_CHECK();
-      double dsum;
-      TOPO_CUDA_CHECK(cudaMemcpyAsync(&dsum, c->dtmp, sizeof(double), cudaMemcpyDeviceToHost, s));
-      TOPO_CUDA_CHECK(cudaStreamSynchronize(s));
-      const double eps = std::max(dsum / n * 1e-8, 1e-14);
-      k_add_diag<<<(n + 255) / 256, 256, 0, s>>>(n, c->C.A, eps);
-      TOPO_LAUNCH_CHECK();
-      bad = dense_cholesky(n, c->C.band, c->C.A, c->C.Dt, c->C.flag, s);
-      if (bad) throw std::runtime_error("coarsest-level Cholesky failed even after eps*I regularisation");
-      c->C.kind = 2;
+    Level& Lc = c->L[c->n_levels - 1];
+    const size_t sb = sizeof(double) * 243 * Lc.g.nnodes;
+    if (!c->coarse_lag || !c->C.have) {
+      coarse_wait_background(c);
+      TOPO_CUDA_CHECK(cudaMemcpyAsync(c->C.cur.S64c, Lc.S64, sb, cudaMemcpyDeviceToDevice, s));
+      TOPO_CUDA_CHECK(cudaEventRecord(c->ev_ph[3], s));
+      slot_launch(c, c->C.cur, s);
+      TOPO_CUDA_CHECK(cudaEventRecord(c->ev_ph[4], s));
+      slot_finish(c, c->C.cur, s);
+      c->C.have = true;
     } else {
-      c->C.kind = 1;
+      // The V-cycle keeps the previous setup's factor; this setup's factor
+      // builds on the background stream and replaces it at the next setup.
+      if (c->C.bg_pending) {
+        TOPO_CUDA_CHECK(cudaEventSynchronize(c->C.bg_done));
+        c->C.bg_pending = false;
+        slot_finish(c, c->C.nxt, s);
+        std::swap(c->C.cur, c->C.nxt);
+      }
+      if (!c->C.nxt.A) alloc_slot(c, c->C.nxt);
+      slot_graph(c, c->C.nxt, s);
+      TOPO_CUDA_CHECK(cudaMemcpyAsync(c->C.nxt.S64c, Lc.S64, sb, cudaMemcpyDeviceToDevice, s));
+      TOPO_CUDA_CHECK(cudaEventRecord(c->C.ev_copy, s));
+      TOPO_CUDA_CHECK(cudaStreamWaitEvent(c->C.bg_stream, c->C.ev_copy, 0));
+      slot_launch(c, c->C.nxt, c->C.bg_stream);
+      TOPO_CUDA_CHECK(cudaEventRecord(c->C.bg_done, c->C.bg_stream));
+      c->C.bg_pending = true;
     }
-    TOPO_CUDA_CHECK(cudaEventRecord(c->ev_ph[4], s));
-    dense_inverse_factor(n, c->C.band, c->C.A, c->C.Dt, c->C.Di, c->C.work, c->C.ldc,
-                         c->vec64 ? c->C.work : nullptr, c->vec64 ? nullptr : c->C.X32, s);
   }
   TOPO_CUDA_CHECK(cudaEventRecord(c->ev_ph[5], s));
   TOPO_CUDA_CHECK(cudaStreamSynchronize(s));
@@ -539,7 +635,7 @@ void pcg_iteration(topo_ctx* c, cudaStream_t s) {
 std::vector<double> pcg_graph_key(const topo_ctx* c) {
   std::vector<double> k = {(double)c->cheb_form, c->lam_safety, c->cheb_lower, (double)c->use_tc,
                            (double)c->fine_degree, (double)c->coarse_degree,
-                           (double)reinterpret_cast<uintptr_t>(c->C.work), (double)reinterpret_cast<uintptr_t>(c->C.X32),
+                           (double)reinterpret_cast<uintptr_t>(c->C.cur.work), (double)reinterpret_cast<uintptr_t>(c->C.cur.X32),
                            (double)reinterpret_cast<uintptr_t>(c->C.y), (double)c->C.n, (double)c->C.ldc};
   for (const Level& Lv : c->L) {
     k.push_back(std::isnan(Lv.lam) ? -1.0 : Lv.lam);  // NaN (no estimate) would never compare equal
@@ -962,6 +1058,9 @@ int topo_ctx_create(int nelx, int nely, int nelz, int n_levels, int mode, int fi
     TOPO_CUDA_CHECK(cudaEventCreateWithFlags(&c->ev_in, cudaEventDisableTiming));
     TOPO_CUDA_CHECK(cudaEventCreateWithFlags(&c->ev_out, cudaEventDisableTiming));
     for (auto& e : c->ev_ph) TOPO_CUDA_CHECK(cudaEventCreate(&e));
+    TOPO_CUDA_CHECK(cudaStreamCreateWithFlags(&c->C.bg_stream, cudaStreamNonBlocking));
+    TOPO_CUDA_CHECK(cudaEventCreateWithFlags(&c->C.ev_copy, cudaEventDisableTiming));
+    TOPO_CUDA_CHECK(cudaEventCreateWithFlags(&c->C.bg_done, cudaEventDisableTiming));
     int nx = nelx, ny = nely, nz = nelz;
     for (int l = 0; l < n_levels; ++l) {
       Level Lv;
@@ -1021,7 +1120,6 @@ int topo_ctx_create(int nelx, int nely, int nelz, int n_levels, int mode, int fi
     c->C.scrA = c->alloc<double>(maxc);
     c->C.scrB = c->alloc<double>(maxc);
     c->C.scrC = c->alloc<double>(maxc);
-    c->C.flag = c->alloc<int>(1);
     *out = c;
     return 0;
   } catch (const std::exception& e) {
@@ -1040,6 +1138,12 @@ int topo_ctx_destroy(topo_ctx* c) {
   if (c->h_st) cudaFreeHost(c->h_st);
   if (c->blk_Gh) cudaFreeHost(c->blk_Gh);
   if (c->pcg_exec) cudaGraphExecDestroy(c->pcg_exec);
+  if (c->C.bg_pending && c->C.bg_done) cudaEventSynchronize(c->C.bg_done);
+  for (FactorSlot* f : {&c->C.cur, &c->C.nxt})
+    if (f->graph) cudaGraphExecDestroy(f->graph);
+  if (c->C.ev_copy) cudaEventDestroy(c->C.ev_copy);
+  if (c->C.bg_done) cudaEventDestroy(c->C.bg_done);
+  if (c->C.bg_stream) cudaStreamDestroy(c->C.bg_stream);
   if (c->ev_in) cudaEventDestroy(c->ev_in);
   if (c->ev_out) cudaEventDestroy(c->ev_out);
   for (auto& e : c->ev_ph)
@@ -1112,18 +1216,16 @@ int topo_set_problem(topo_ctx* c, const uint8_t* free_mask, const double* F, voi
             }
         }
       }
-      if (c->C.n != n || c->C.A == nullptr) {
+      coarse_wait_background(c);
+      c->C.have = false;
+      if (c->C.n != n || c->C.cur.A == nullptr) {
         c->C.n = n;
         c->C.dof_index = c->alloc<int>(Lc.g.ndof);
         c->C.free_list = c->alloc<int>(std::max(n, 1));
-        const long long nt = (n + 31) / 32;
-        c->C.ldc = nt * 32;
-        c->C.A = c->alloc<double>((long long)n * n);
-        c->C.Dt = c->alloc<double>(nt * 1024);
-        c->C.Di = c->alloc<double>(nt * 1024);
-        c->C.work = c->alloc<double>((long long)n * c->C.ldc);
-        if (!c->vec64) c->C.X32 = c->alloc<float>((long long)n * c->C.ldc);
+        c->C.ldc = ((n + 31) / 32) * 32;
         c->C.y = c->alloc<double>(std::max(n, 1));
+        alloc_slot(c, c->C.cur);
+        if (c->C.nxt.A) alloc_slot(c, c->C.nxt);
         dense_apply_prepare(n);
       }
       c->C.band = band;
@@ -1229,6 +1331,16 @@ int topo_fgmres(topo_ctx* c, const void* b, void* x, double tol, int maxiter, in
     if (maxiter < 1 || restart < 1) throw std::invalid_argument("topo_fgmres: maxiter and restart must be >= 1");
     StreamGuard sg(c, stream);
     return do_fgmres(c, (const double*)b, (double*)x, tol, maxiter, restart, out_iters, out_relres, c->cs);
+  } catch (const std::exception& e) {
+    return fail(c, e);
+  }
+}
+
+int topo_set_coarse_lag(topo_ctx* c, int on) {
+  try {
+    if (!c) throw std::invalid_argument("topo_set_coarse_lag: null context");
+    c->coarse_lag = on != 0;
+    return 0;
   } catch (const std::exception& e) {
     return fail(c, e);
   }
@@ -1362,7 +1474,7 @@ int topo_gmg_info(topo_ctx* c, long long* n_free, double* lambda_max, int* coars
       }
       if (lambda_max) lambda_max[l] = c->L[l].lam;
     }
-    if (coarse_kind) *coarse_kind = c->C.kind;
+    if (coarse_kind) *coarse_kind = c->C.cur.kind;
     return 0;
   } catch (const std::exception& e) {
     return fail(c, e);

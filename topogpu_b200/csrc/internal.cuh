@@ -242,6 +242,8 @@ void dense_assemble(const Grid& g, const double* S, const int* dof_index, int n,
 // factored diagonal blocks in Dt); returns 0 on success, 1 if a pivot was not
 // positive/finite (host sync inside).
 int dense_cholesky(int n, int band, double* A, double* Dt, int* flag, cudaStream_t s);
+// the same launches without the flag read-back (capturable; flag checked later)
+void dense_cholesky_launch(int n, int band, double* A, double* Dt, int* flag, cudaStream_t s);
 // W = L^-1 into W64 (FP64, lower) and into the apply matrices C64/C32 (W
 // lower, W^T upper); Di receives the inverses of the diagonal blocks.
 void dense_inverse_factor(int n, int band, const double* A, const double* Dt, double* Di, double* W64,

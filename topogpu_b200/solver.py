@@ -74,7 +74,8 @@ class SIMPSolver:
 
     def __init__(self, backend="cuda", linear_solver="auto", optimizer="oc", tol=1.0e-5, max_krylov=800,
                  max_iter=12, move=0.10, rho_min=1.0e-3, *, precision="mixed", levels=4, fine_degree=2,
-                 coarse_degree=2, use_filter=False, penal=3.0, smoother="chebyshev", device=None):
+                 coarse_degree=2, use_filter=False, penal=3.0, smoother="chebyshev", coarse_lag=None,
+                 device=None):
         if optimizer != "oc":
             raise ValueError("Only optimizer='oc' is implemented in v0.1.0.")
         if backend in {"cpu", "scipy"}:
@@ -94,6 +95,10 @@ class SIMPSolver:
         self.use_filter = use_filter
         self.penal = penal
         self.smoother = smoother
+        # one-setup-lagged coarsest factor built in the background: off by default
+        # (on the 1M-element SIMP run it saved the factorisation time but cost as
+        # much in extra PCG iterations and in contention with the Krylov kernels)
+        self.coarse_lag = bool(coarse_lag) if coarse_lag is not None else False
         self.device = device
 
     def make_state_solver(self, problem: TopologyProblem) -> StateSolver:
@@ -103,9 +108,11 @@ class SIMPSolver:
         bc = generate_bc(spec)
         F = problem.force_override if problem.force_override is not None else bc.F
         outer = "fgmres" if self.linear_solver == "fgmres_gmg" else "pcg"
-        return StateSolver(problem.nel, bc.free_mask(), F, n_levels=self.levels, precision=self.precision,
-                           fine_degree=self.fine_degree, coarse_degree=self.coarse_degree, outer=outer,
-                           tol=self.tol, maxiter=self.max_krylov, smoother=self.smoother, device=self.device)
+        st = StateSolver(problem.nel, bc.free_mask(), F, n_levels=self.levels, precision=self.precision,
+                         fine_degree=self.fine_degree, coarse_degree=self.coarse_degree, outer=outer,
+                         tol=self.tol, maxiter=self.max_krylov, smoother=self.smoother, device=self.device)
+        st.ctx.set_coarse_lag(self.coarse_lag)
+        return st
 
     def solve(self, problem: TopologyProblem) -> OptimizationResult:
         problem.validate()
