@@ -201,13 +201,20 @@ k_stencil(Grid g, const TC* __restrict__ S, const T* __restrict__ u, const uint8
   if (n >= g.nnodes) return;
   int ix, iy, iz;
   node_xyz(g, n, ix, iy, iz);
+  // clamped neighbour coordinates (out-of-grid couplings have zero
+  // coefficients, so any in-grid value serves) and the nine row bases
+  const int jxs[3] = {max(ix - 1, 0), ix, min(ix + 1, g.NX - 1)};
+  const int jys[3] = {max(iy - 1, 0), iy, min(iy + 1, g.NY - 1)};
+  const int jzs[3] = {max(iz - 1, 0), iz, min(iz + 1, g.NZ - 1)};
+  long long rb[9];
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int b = 0; b < 3; ++b) rb[a * 3 + b] = ((long long)jxs[a] * g.NY + jys[b]) * g.NZ;
   T a0 = 0, a1 = 0, a2 = 0;
 #pragma unroll
   for (int k = 0; k < 27; ++k) {
-    const int jx = min(max(ix + k / 9 - 1, 0), g.NX - 1);
-    const int jy = min(max(iy + (k / 3) % 3 - 1, 0), g.NY - 1);
-    const int jz = min(max(iz + k % 3 - 1, 0), g.NZ - 1);
-    const long long j = ((long long)jx * g.NY + jy) * g.NZ + jz;
+    const long long j = rb[k / 3] + jzs[k % 3];
     T uj[3];
 #pragma unroll
     for (int d = 0; d < 3; ++d) {

@@ -85,30 +85,40 @@ k_level0(Grid g, const TU* __restrict__ u, const T* __restrict__ E, const uint8_
   const int tid = threadIdx.x + TZ * (threadIdx.y + TY * threadIdx.z);
   constexpr int NT = TX * TY * TZ;
 
-  // stage nodal values of the brick + halo (zero outside the grid)
-  for (int idx = tid; idx < UX * UY * UZ * 3; idx += NT) {
-    const int c = idx % 3;
-    const int zz = (idx / 3) % UZ;
-    const int yy = (idx / (3 * UZ)) % UY;
-    const int xx = idx / (3 * UZ * UY);
-    const int gx = x0 - 1 + xx, gy = y0 - 1 + yy, gz = z0 - 1 + zz;
-    TS v = 0;
-    if (gx >= 0 && gx < g.NX && gy >= 0 && gy < g.NY && gz >= 0 && gz < g.NZ) {
-      const long long n = ((long long)gx * g.NY + gy) * g.NZ + gz;
-      v = load_as<TS>(u + 3 * n + c);
-      if constexpr (BF) v = __bfloat162float(__float2bfloat16_rn((float)v));
+  // stage nodal values of the brick + halo (zero outside the grid). A node
+  // column (xx, yy) is one contiguous z-run of 3*UZ values in global memory:
+  // warp w copies columns w, w + 8, ... with its lanes along the run, so the
+  // loads coalesce and the index arithmetic is one division by 3.
+  {
+    const int warp = tid >> 5, lane = tid & 31;
+    for (int col = warp; col < UX * UY; col += NT / 32) {
+      const int xx = col / UY, yy = col - UY * xx;
+      const int gx = x0 - 1 + xx, gy = y0 - 1 + yy;
+      const bool cin = gx >= 0 && gx < g.NX && gy >= 0 && gy < g.NY;
+      const long long base = 3 * (((long long)gx * g.NY + gy) * g.NZ + (z0 - 1));
+#pragma unroll
+      for (int e = lane; e < 3 * UZ; e += 32) {
+        const int zz = e / 3, c = e - 3 * zz;
+        const int gz = z0 - 1 + zz;
+        TS v = 0;
+        if (cin && gz >= 0 && gz < g.NZ) {
+          v = load_as<TS>(u + base + e);
+          if constexpr (BF) v = __bfloat162float(__float2bfloat16_rn((float)v));
+        }
+        us[xx][yy][zz][c] = v;
+      }
     }
-    us[xx][yy][zz][c] = v;
-  }
-  for (int idx = tid; idx < EX * EY * EZ; idx += NT) {
-    const int zz = idx % EZ;
-    const int yy = (idx / EZ) % EY;
-    const int xx = idx / (EZ * EY);
-    const int gx = x0 - 1 + xx, gy = y0 - 1 + yy, gz = z0 - 1 + zz;
-    TS v = 0;
-    if (gx >= 0 && gx < g.nx && gy >= 0 && gy < g.ny && gz >= 0 && gz < g.nz)
-      v = (TS)E[((long long)gx * g.ny + gy) * g.nz + gz];
-    es[xx][yy][zz] = v;
+    // moduli of the incident elements: element columns are contiguous z-runs too
+    for (int col = warp; col < EX * EY; col += NT / 32) {
+      const int xx = col / EY, yy = col - EY * xx;
+      const int gx = x0 - 1 + xx, gy = y0 - 1 + yy;
+      const bool cin = gx >= 0 && gx < g.nx && gy >= 0 && gy < g.ny;
+      const long long base = ((long long)gx * g.ny + gy) * g.nz + (z0 - 1);
+      for (int zz = lane; zz < EZ; zz += 32) {
+        const int gz = z0 - 1 + zz;
+        es[xx][yy][zz] = (cin && gz >= 0 && gz < g.nz) ? (TS)E[base + zz] : (TS)0;
+      }
+    }
   }
   __syncthreads();
 
