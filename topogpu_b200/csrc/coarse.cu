@@ -490,6 +490,7 @@ __global__ void __launch_bounds__(128) k_chol_step(int n, int k, int band, doubl
   __shared__ double W[CNB][CNB + 1];
   __shared__ double L[CNB][CNB + 1];
   __shared__ double invd[CNB];
+  __shared__ double colj[CNB + 1];  // column j of the pivot step, then rsqrt(d)
   const int nb = min(CNB, n - k);
   const int tid = threadIdx.x;
   for (int q = tid; q < CNB * CNB; q += blockDim.x) {
@@ -497,35 +498,49 @@ __global__ void __launch_bounds__(128) k_chol_step(int n, int k, int band, doubl
     W[i][j] = (i < nb && j < nb && j <= i) ? A[(long long)(k + i) * n + k + j] : (i == j ? 1.0 : 0.0);
   }
   __syncthreads();
-  // thread -> 8 entries of the block: rows r0 + 4m (m < 8), column cc
-  const int cc = tid & 31, r0 = tid >> 5;
+  // warp 0 factors with lane cc holding column cc of the block in
+  // registers. Per pivot j (fully unrolled, so register indices are
+  // compile-time): lane j evaluates rsqrt(d) once and publishes its column in
+  // shared memory; every lane then reads that column with broadcast loads
+  // (no read-after-write through shared memory inside the update) and
+  // updates its own column in registers.
   bool bad = false;
-#pragma unroll 1
-  for (int j = 0; j < CNB; ++j) {
-    const double d = W[j][j];
-    const bool ok = d > 0.0 && isfinite(d);
-    bad |= !ok;
-    const double dd = ok ? d : 1.0;
-    const double inv_d = 1.0 / dd, rs = rsqrt(dd);
-    if (cc == j) {
+  if (tid < 32) {
+    const int lane = tid;
+    double wc[CNB];
 #pragma unroll
-      for (int m = 0; m < 8; ++m) {
-        const int i = r0 + 4 * m;
-        if (i == j) L[i][j] = sqrt(dd);
-        else if (i > j) L[i][j] = W[i][j] * rs;
-        else L[i][j] = 0.0;
-      }
-      if (r0 == 0) invd[j] = rs;
-    } else if (cc > j) {
-      const double wcj = W[cc][j] * inv_d;
+    for (int i = 0; i < CNB; ++i) wc[i] = W[i][lane];
 #pragma unroll
-      for (int m = 0; m < 8; ++m) {
-        const int i = r0 + 4 * m;
-        if (i >= cc) W[i][cc] -= W[i][j] * wcj;
+    for (int j = 0; j < CNB; ++j) {
+      if (lane == j) {
+        const double d = wc[j];
+        const bool ok = d > 0.0 && isfinite(d);
+        const double dd = ok ? d : 1.0;
+        const double rs = rsqrt(dd);
+        colj[CNB] = rs;
+        bad |= !ok;
+#pragma unroll
+        for (int i = j + 1; i < CNB; ++i) colj[i] = wc[i];
+        L[j][j] = dd * rs;
+        invd[j] = rs;
       }
+      __syncwarp();
+      const double rs = colj[CNB];
+      if (lane > j) {
+        const double lj = colj[lane];
+        L[lane][j] = lj * rs;
+        const double w = lj * (rs * rs);
+#pragma unroll
+        for (int i = j + 1; i < CNB; ++i)
+          if (i >= lane) wc[i] -= colj[i] * w;
+      } else if (lane < j) {
+        L[lane][j] = 0.0;
+      }
+      __syncwarp();
     }
-    __syncthreads();
+    bad = __any_sync(0xffffffffu, bad);
   }
+  __syncthreads();
   if (blockIdx.x == 0) {
     double* D = Dt + (long long)(k / CNB) * CNB * CNB;
     for (int q = tid; q < CNB * CNB; q += blockDim.x) D[q] = (q % CNB <= q / CNB) ? L[q / CNB][q % CNB] : 0.0;
