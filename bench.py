@@ -248,6 +248,51 @@ def cpu_baseline(sample_nel=(48, 24, 24), steps=3):
                        f"rate scaled to 1,024,000 elements by element count")}
 
 
+def extras():
+    """Multi-load block PCG (96x48x48, 8 seeded point loads) and 64 batched
+    uneven cantilevers, both mixed precision at rtol 1e-5, device-synchronised
+    wall time after a warm-up call."""
+    from topogpu_b200.batch import BatchSolver, config4b_meshes, summarize
+    from topogpu_b200.bc import cantilever_edge_load, face_point_loads
+    from topogpu_b200.state import StateSolver
+
+    out = {}
+    nel = (96, 48, 48)
+    mask, F = cantilever_edge_load(nel)
+    rho = np.random.default_rng(31).uniform(0.05, 1.0, int(np.prod(nel)))
+    B = face_point_loads(nel, 8, 32)
+    st = StateSolver(nel, mask, F, n_levels=4, precision="mixed", tol=1e-5, maxiter=800, fine_degree=3)
+    st.solve_block(rho, B)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    comps, _ = st.solve_block(rho, B)
+    torch.cuda.synchronize()
+    t_block = time.perf_counter() - t0
+    it_block = st.last_cg_iters
+    t0 = time.perf_counter()
+    its = 0
+    for j in range(8):
+        x = torch.zeros(st.ctx.ndof, dtype=torch.float64, device="cuda")
+        i1, _, _ = st.ctx.pcg(torch.tensor(B[j] * mask, device="cuda"), x, 1e-5, 800)
+        its += i1
+    torch.cuda.synchronize()
+    t_single = time.perf_counter() - t0
+    st.close()
+    out["block_pcg_96x48x48_8loads"] = {"block_ms": t_block * 1e3, "block_iters": it_block,
+                                        "single_ms_total": t_single * 1e3, "single_iters_total": its,
+                                        "speedup": t_single / t_block}
+    meshes = config4b_meshes(64, seed=0)
+    rng = np.random.default_rng(41)
+    rhos = [torch.tensor(rng.uniform(0.05, 1.0, int(np.prod(m))), dtype=torch.float64, device="cuda")
+            for m in meshes]
+    bs = BatchSolver(meshes, precision="mixed", tol=1e-5)
+    tune = bs.autotune(rhos)
+    res = bs.solve(rhos)
+    out["batched_64_uneven_cantilevers"] = {**summarize(res), "autotune_trials": tune["trials"]}
+    bs.close()
+    return out
+
+
 def reference_arm(args, rank):
     if rank != 0:
         return 0
@@ -291,6 +336,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp32", action="store_true")
+    ap.add_argument("--no-extras", action="store_true", help="skip the multi-load and batched-mesh measurements")
     ap.add_argument("--micro-reps", type=int, default=100)
     ap.add_argument("--only-ku", action="store_true", help="run only the K.u microbenchmark (profiling)")
     ap.add_argument("--only-simp", action="store_true", help="run only the mixed SIMP steps (profiling)")
@@ -390,6 +436,8 @@ def main():
         line["mixed_speedup_vs_fp32"] = line["plain_fp32"]["ms_per_step"] / ms_step
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline()
+    if world == 1 and not args.no_extras:
+        line["extras"] = extras()
     if rank == 0:
         print(json.dumps(line))
     if dist:

@@ -12,22 +12,13 @@ import pytest
 import torch
 
 from oracle import fem
+from topogpu_b200.bc import face_point_loads
 from topogpu_b200.context import TopoContext
 from topogpu_b200.state import StateSolver
 
 
 def point_loads(nel, k, seed):
-    """k unit point loads at distinct random nodes of the x = nelx face, random unit directions."""
-    nx, ny, nz = nel
-    rng = np.random.default_rng(seed)
-    face = ((nx * (ny + 1) + np.arange(ny + 1)[:, None]) * (nz + 1) + np.arange(nz + 1)[None, :]).ravel()
-    nodes = rng.choice(face, k, replace=False)
-    dirs = rng.normal(size=(k, 3))
-    dirs /= np.linalg.norm(dirs, axis=1, keepdims=True)
-    B = np.zeros((k, fem.n_dof(nel)))
-    for j in range(k):
-        B[j, 3 * nodes[j]:3 * nodes[j] + 3] = dirs[j]
-    return B
+    return face_point_loads(nel, k, seed)
 
 
 def _rho(n, seed):

@@ -125,3 +125,20 @@ def cantilever_edge_load(nel, total: float = -1.0):
     edge = (nx * (ny + 1) + np.arange(ny + 1)) * (nz + 1)
     F[3 * edge + 2] = total / len(edge)
     return mask, F
+
+
+def face_point_loads(nel, k, seed):
+    """k unit point loads at distinct random nodes of the x = nelx face, in
+    random unit directions (seeded): the load cases of the multi-load
+    benchmark. Returns a (k, ndof) float64 array."""
+    nx, ny, nz = (int(v) for v in nel)
+    rng = np.random.default_rng(seed)
+    face = ((nx * (ny + 1) + np.arange(ny + 1)[:, None]) * (nz + 1) + np.arange(nz + 1)[None, :]).ravel()
+    nodes = rng.choice(face, k, replace=False)
+    dirs = rng.normal(size=(k, 3))
+    dirs /= np.linalg.norm(dirs, axis=1, keepdims=True)
+    B = np.zeros((k, 3 * (nx + 1) * (ny + 1) * (nz + 1)))
+    for j in range(k):
+        B[j, 3 * nodes[j]:3 * nodes[j] + 3] = dirs[j]
+    return B
+
