@@ -248,6 +248,20 @@ def cpu_baseline(sample_nel=(48, 24, 24), steps=3):
                        f"rate scaled to 1,024,000 elements by element count")}
 
 
+def max_over_ranks(x: float, dist, device="cuda") -> float:
+    """Max of a per-rank time over all ranks (the slowest rank sets the job time)."""
+    if dist is None:
+        return float(x)
+    t = torch.tensor([float(x)], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_rate(world: int, ms_per_step: float) -> float:
+    """Whole-job SIMP iterations/s of `world` independent replicas."""
+    return world * 1e3 / ms_per_step
+
+
 def extras():
     """Multi-load block PCG (96x48x48, 8 seeded point loads) and 64 batched
     uneven cantilevers, both mixed precision at rtol 1e-5, device-synchronised
@@ -381,20 +395,12 @@ def main():
     launches = mixed["launches"]
     clk = clocks.stop()
     torch.cuda.synchronize()
-    total_ms = sum(mixed["ms"])
-    if dist:
-        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(sum(mixed["ms"]), dist)
     ms_step = total_ms / args.steps
-    value = world * 1e3 / ms_step
+    value = replica_rate(world, ms_step)
     fp32 = None if args.no_fp32 else simp_steps("fp32", args.steps, args.warmup, flush)
     e2e = e2e_steps("mixed", args.steps, args.warmup, flush)
-    e2e_ms = sum(e2e["ms"])
-    if dist:
-        t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(sum(e2e["ms"]), dist)
     rel_err = fp64_compliance_check()
     del n0
 
@@ -429,7 +435,7 @@ def main():
             "roofline": roof,
             "clocks": clk,
             "gpu_launches": launches,
-            "e2e": {"value": world * 1e3 / (e2e_ms / args.steps), "unit": UNIT,
+            "e2e": {"value": replica_rate(world, e2e_ms / args.steps), "unit": UNIT,
                     "h2d_bytes_per_step": e2e["h2d"], "d2h_bytes_per_step": e2e["d2h"]},
             "gmg": mixed["gmg"]}
     if fp32 is not None:
