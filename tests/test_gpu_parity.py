@@ -346,3 +346,43 @@ def test_lagged_coarse_factor_same_solutions(cuda_dev):
         out[lag] = np.array(comps)
         st.close()
     assert np.max(np.abs(out[True] - out[False]) / np.abs(out[False])) < 1e-5
+
+
+@pytest.mark.gpu
+def test_probe_quality_and_kappa_eff_match_oracle(cuda_dev):
+    """probe_quality and the Lanczos kappa_eff of M K (multigrid_v4.py:606-655,
+    821-832) on the reference V-cycle, against the same Lanczos run on the
+    oracle hierarchy with the same start vector."""
+    from topogpu_b200.state import StateSolver
+
+    g = load_golden("galerkin")
+    tag, nel, nlev = "24x12x6", (24, 12, 6), 4
+    bc = fem.cantilever_bc(nel)
+    mask = np.zeros(bc.ndof, dtype=np.uint8)
+    mask[bc.free] = 1
+    st = StateSolver(nel, mask, bc.F, n_levels=nlev, precision="fp64", smoother="reference", probe=True,
+                     tol=1e-8, device=DEV)
+    rho = g[f"rho_{tag}"]
+    st.solve(rho)
+    q = st.last_multigrid_quality
+    assert q["finite"] and q["pd"] and q["z_norm"] > 0 and q["jacobi_norm"] > 0
+    kappa = st.estimate_kappa_eff(30)
+    # oracle: same start vector (torch generator, seed 0), compact free vectors
+    h = gmg.GMG(nel, bc.free, n_levels=nlev, fine_prec="fp64", fine_degree=2).setup(fem.simp_modulus(rho))
+    v = (torch.randn(bc.ndof, generator=torch.Generator().manual_seed(0), dtype=torch.float64).numpy())[bc.free]
+    v /= np.linalg.norm(v)
+    vp = np.zeros_like(v)
+    al, be = [], []
+    for j in range(30):
+        w = h.apply(h.fine_op64(v))
+        a = float(v @ w)
+        al.append(a)
+        w = w - a * v - (be[-1] * vp if j > 0 else 0.0)
+        if j < 29:
+            b = float(np.linalg.norm(w))
+            be.append(b)
+            vp, v = v, w / b
+    eig = np.linalg.eigvalsh(np.diag(al) + np.diag(be, 1) + np.diag(be, -1))
+    ref = eig[-1] / eig[eig > 0][0]
+    assert abs(kappa - ref) <= 1e-6 * ref, (kappa, ref)
+    st.close()

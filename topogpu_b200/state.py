@@ -29,7 +29,7 @@ class StateSolver:
 
     def __init__(self, nel, free_mask, F, *, n_levels=4, precision="mixed", fine_degree=2, coarse_degree=2,
                  cheb_lower=1.0 / 30.0, outer="pcg", restart=32, tol=1e-5, maxiter=800, warm_start=True,
-                 E0=1.0, Emin=1e-9, dense_max=16384, smoother="chebyshev", device=None):
+                 E0=1.0, Emin=1e-9, dense_max=16384, smoother="chebyshev", probe=False, device=None):
         if outer not in ("pcg", "fgmres"):
             raise ValueError(f"outer must be 'pcg' or 'fgmres', got {outer!r}")
         self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
@@ -57,6 +57,8 @@ class StateSolver:
         self.last_converged = False
         self.last_outer_solver = outer
         self.last_timing: dict = {}
+        self.probe = probe  # one extra V-cycle per solve for last_multigrid_quality
+        self.last_multigrid_quality: dict = {}
 
     def _krylov(self):
         if self.outer == "pcg":
@@ -79,6 +81,8 @@ class StateSolver:
         self.ctx.gmg_setup(self.E)
         if timing:
             ev[1].record()
+        if self.probe:
+            self.last_multigrid_quality = self.probe_quality()
         warm = self.warm_start and self._have_prev
         if not warm:
             self.u.zero_()
@@ -117,6 +121,53 @@ class StateSolver:
         self.last_outer_solver = "block_pcg"
         Bm = B * self.free_mask
         return [float(torch.dot(Bm[j], U[j])) for j in range(B.shape[0])], U
+
+    # -- diagnostics (GalerkinMatFreeGMG.probe_quality / estimate_kappa_eff) --
+    def _precondition(self, r):
+        vdt = self.ctx.vec_dtype
+        return self.ctx.gmg_apply(r.to(vdt).contiguous()).to(torch.float64)
+
+    def probe_quality(self, rhs=None) -> dict:
+        """One V-cycle on rhs (default: the load) with the current hierarchy:
+        finiteness, positivity of rhs.z and the norms of z and of the Jacobi
+        step, as GalerkinMatFreeGMG.probe_quality (multigrid_v4.py:821-832)."""
+        rhs = (self.F * self.free_mask) if rhs is None else rhs.to(torch.float64) * self.free_mask
+        z = self._precondition(rhs)
+        d = self.ctx.diag(self.E)
+        zj = torch.where(self.free_mask.bool(), rhs / d, torch.zeros_like(rhs))
+        return {"finite": bool(torch.isfinite(z).all()), "pd": float(torch.dot(rhs, z)) > 0.0,
+                "z_norm": float(z.norm()), "jacobi_norm": float(zj.norm())}
+
+    def estimate_kappa_eff(self, n_iter: int = 30, seed: int = 0) -> float:
+        """lambda_max / lambda_min of the n_iter-step Lanczos tridiagonal of the
+        preconditioned operator M K on the current hierarchy (Euclidean inner
+        product, seeded normal start vector), as
+        GalerkinMatFreeGMG.estimate_kappa_eff (multigrid_v4.py:606-655)."""
+        g = torch.Generator().manual_seed(seed)
+        m = self.free_mask.to(torch.float64)
+        v = torch.randn(self.ctx.ndof, generator=g, dtype=torch.float64).to(self.device) * m
+        v /= v.norm()
+        v_prev = torch.zeros_like(v)
+        alphas, betas = [], []
+        for j in range(n_iter):
+            w = self._precondition(self.ctx.matvec(v, self.E))
+            a = float(torch.dot(v, w))
+            alphas.append(a)
+            w = w - a * v
+            if j > 0:
+                w = w - betas[-1] * v_prev
+            if j < n_iter - 1:
+                b = float(w.norm())
+                if b < 1e-14:
+                    break
+                betas.append(b)
+                v_prev, v = v, w / b
+        betas = betas[: len(alphas) - 1]
+        T = np.diag(alphas) + np.diag(betas, 1) + np.diag(betas, -1)
+        eig = np.linalg.eigvalsh(T)
+        eig = eig[eig > 0]
+        self.last_kappa_eff = float(eig[-1] / max(eig[0], 1e-300)) if len(eig) else float("nan")
+        return self.last_kappa_eff
 
     def reset_warm_start(self):
         """Make the next solve start from u = 0."""
