@@ -124,6 +124,51 @@ def oc_update_filtered(rho, dc, dv, volfrac, move, H, rho_min=1e-3):
     return rn, k + 1
 
 
+def heaviside(rho_f, beta, eta):
+    """Smoothed Heaviside projection of run_simp (pub_simp_solver.py:245-248):
+    (tanh(b e) + tanh(b (x - e))) / (tanh(b e) + tanh(b (1 - e))); identity
+    for beta < 1e-6."""
+    rho_f = np.asarray(rho_f, dtype=np.float64)
+    if beta < 1e-6:
+        return rho_f.copy()
+    return (np.tanh(beta * eta) + np.tanh(beta * (rho_f - eta))) / (np.tanh(beta * eta) + np.tanh(beta * (1.0 - eta)))
+
+
+def heaviside_deriv(rho_f, beta, eta):
+    """d heaviside / d rho_f (pub_simp_solver.py:250-253)."""
+    rho_f = np.asarray(rho_f, dtype=np.float64)
+    if beta < 1e-6:
+        return np.ones_like(rho_f)
+    denom = np.tanh(beta * eta) + np.tanh(beta * (1.0 - eta))
+    return beta * (1.0 - np.tanh(beta * (rho_f - eta)) ** 2) / denom
+
+
+def oc_update_projected(rho, dc, dv, volfrac, move, H, beta, eta, rho_min=1e-3):
+    """run_simp's OC with the volume measured after filter AND Heaviside
+    projection (pub_simp_solver.py:319-340 with use_heaviside and beta >
+    1e-6): l1=0, l2=1e9, <=100 bisections, stop when l2-l1 < 1e-9. Returns
+    (candidate, n_eval)."""
+    rho = np.asarray(rho, dtype=np.float64)
+    dcs = np.minimum(dc, -1e-12)
+    dvs = np.maximum(dv, 1e-12)
+    n = len(rho)
+    l1, l2 = 0.0, 1e9
+    rn = None
+    k = 0
+    for k in range(100):
+        lm = 0.5 * (l1 + l2)
+        rn = rho * np.sqrt(-dcs / (lm * dvs))
+        rn = np.clip(rn, rho - move, rho + move)
+        rn = np.clip(rn, rho_min, 1.0)
+        if heaviside(H @ rn, beta, eta).sum() / n > volfrac:
+            l1 = lm
+        else:
+            l2 = lm
+        if l2 - l1 < 1e-9:
+            break
+    return rn, k + 1
+
+
 def grayness(rho) -> float:
     """4 mean(rho(1-rho)) (topogpu/solver.py:120-121)."""
     rho = np.asarray(rho)

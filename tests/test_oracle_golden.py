@@ -131,3 +131,16 @@ def test_known_answers_from_survey():
     bc = fem.cantilever_bc(nel)
     u = fem.direct_solve(fem.simp_modulus(np.full(1728, 0.3)), nel, bc)
     assert abs(bc.F @ u - 399.9508808170127) < 1e-9
+
+
+def test_heaviside_restatement_matches_reference_formulas():
+    """The projection and its derivative against a central difference, and
+    the beta -> 0 identity (pub_simp_solver.py:245-253)."""
+    x = np.linspace(0.0, 1.0, 101)
+    for beta in (1.0, 8.0, 32.0):
+        h = design.heaviside(x, beta, 0.5)
+        assert abs(h[0]) < 1e-15 and abs(h[-1] - 1.0) < 1e-15
+        eps = 1e-6
+        fd = (design.heaviside(x + eps, beta, 0.5) - design.heaviside(x - eps, beta, 0.5)) / (2 * eps)
+        np.testing.assert_allclose(design.heaviside_deriv(x, beta, 0.5), fd, rtol=1e-6, atol=1e-8)
+    assert np.array_equal(design.heaviside(x, 0.0, 0.5), x)
