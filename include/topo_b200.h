@@ -196,6 +196,22 @@ int topo_oc_filtered(topo_ctx* ctx, const double* rho, const double* dc, const d
                      const double* colsum, double volfrac, double move, double rho_min, double* out,
                      int* out_evals, void* stream);
 
+/* Smoothed Heaviside projection of run_simp (src/gpu_fem/pub_simp_solver.py:
+ * 245-253) over the ctx's n_elem elements: phys = h(rho_f), dh = h'(rho_f)
+ * (either output may be NULL, not both); the identity (phys = rho_f, dh = 1)
+ * unless beta > 1e-6, the guard of every run_simp call site (331, 348, 366). */
+int topo_heaviside(topo_ctx* ctx, const double* rho_f, double beta, double eta, double* phys,
+                   double* dh, void* stream);
+
+/* Projected-volume OC of run_simp with use_heaviside (src/gpu_fem/
+ * pub_simp_solver.py:319-340): l1=0, l2=1e9, <=100 bisections until
+ * l2-l1<1e-9; the volume of a candidate is sum(h(H cand))/n with H the
+ * linear-hat filter of radius rmin. out must not alias rho, dc or dv; it is
+ * the candidate of the last evaluated lambda. */
+int topo_oc_projected(topo_ctx* ctx, double rmin, const double* rho, const double* dc,
+                      const double* dv, double beta, double eta, double volfrac, double move,
+                      double rho_min, double* out, int* out_evals, void* stream);
+
 /* Bisection OC update that allocates no device memory: the same update as
  * topo_oc, without a context. This entry point has no counterpart in the
  * reference. It is for callers that cannot let a library call cudaMalloc:

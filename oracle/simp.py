@@ -91,21 +91,28 @@ def simp_projected(nel, bc, volfrac, rmin, max_iter, beta, eta=0.5, move=0.2, pe
     """``run_simp`` main loop with Heaviside projection at a fixed beta
     (_fea_and_sensitivity, pub_simp_solver.py:342-377): rho_phys =
     heaviside(H rho), direct solve, dc chained through dh and H^T, dv = H^T dh,
-    OC with the projected volume. Returns (rho_design, compliance history)."""
+    OC with the projected volume. Returns (rho_design, compliance history,
+    final compliance, final rho_phys) like ``simp_filtered``."""
     H = design.filter_matrix(nel, rmin)
     n = H.shape[0]
     rho = np.full(n, float(volfrac))
     hist = []
-    for _ in range(max_iter):
-        rf = H @ rho
+
+    def fea(r):
+        rf = H @ r
         rp = design.heaviside(rf, beta, eta)
         E = 1e-9 + (1.0 - 1e-9) * rp**penal
         U = fem.direct_solve(E, nel, bc)
-        hist.append(float(bc.F @ U))
         dcp = -penal * (1.0 - 1e-9) * rp ** (penal - 1) * fem.element_energy(U, nel)
         dh = design.heaviside_deriv(rf, beta, eta)
-        rho, _ = design.oc_update_projected(rho, H.T @ (dcp * dh), H.T @ dh, volfrac, move, H, beta, eta)
-    return rho, hist
+        return float(bc.F @ U), rp, H.T @ (dcp * dh), H.T @ dh
+
+    for _ in range(max_iter):
+        c, rp, dcd, dvd = fea(rho)
+        hist.append(c)
+        rho, _ = design.oc_update_projected(rho, dcd, dvd, volfrac, move, H, beta, eta)
+    cf, rpf, _, _ = fea(rho)
+    return rho, hist, cf, rpf
 
 
 def simp_filtered(nel, bc, volfrac, rmin, max_iter, move=0.2, penal=3.0, solve=None):

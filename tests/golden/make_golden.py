@@ -21,6 +21,11 @@ reference. Every array is produced by reference code paths:
   oc.npz           topogpu.solver._oc_update on seeded inputs
   filter.npz       _build_density_filter (rmin 1.5, 2.0), DensityFilter.matrix
   run_simp.npz     run_simp config 0 (rmin 1.5, move 0.2, no Heaviside)
+  run_simp_heaviside.npz  run_simp on the same mesh with Heaviside
+                   projection at beta 1 (the SIMPParams default) and beta 8
+
+``python make_golden.py [REF_ROOT] [--only heaviside]`` regenerates all
+fixtures, or only the Heaviside ones.
 """
 
 from __future__ import annotations
@@ -217,8 +222,36 @@ def main(ref_root: str) -> None:
     res = run_simp(params, verbose=False, bc_override=lambda a, b, c: (fixed, free, F))
     np.savez_compressed(HERE / "run_simp.npz", compliance=np.array(res["compliance_history"]),
                         final=np.array(res["final_compliance"]), rho_final=res["rho_final"])
+    heaviside_fixtures(ref_root)
     print("golden fixtures written to", HERE)
 
 
+def heaviside_fixtures(ref_root) -> None:
+    _setup(Path(ref_root))
+    from gpu_fem.pub_simp_solver import SIMPParams, run_simp
+
+    nel = (24, 12, 6)
+    fixed, free, F, ndof = cantilever_bc(nel)
+    d = {}
+    for beta in (1.0, 8.0):
+        params = SIMPParams(nelx=24, nely=12, nelz=6, volfrac=0.3, rmin=1.5, move=0.2, max_iter=3, min_iter=3,
+                            use_heaviside=True, beta_init=beta, eta=0.5)
+        with redirect_stdout(io.StringIO()):
+            res = run_simp(params, verbose=False, bc_override=lambda a, b, c: (fixed, free, F))
+        tag = f"b{int(beta)}"
+        d[f"compliance_{tag}"] = np.array(res["compliance_history"])
+        d[f"rho_final_{tag}"] = res["rho_final"]
+    np.savez_compressed(HERE / "run_simp_heaviside.npz", **d)
+
+
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    import argparse
+
+    ap = argparse.ArgumentParser()
+    ap.add_argument("ref_root", nargs="?", default="/root/reference")
+    ap.add_argument("--only", choices=["heaviside"], default=None)
+    a = ap.parse_args()
+    if a.only == "heaviside":
+        heaviside_fixtures(a.ref_root)
+    else:
+        main(a.ref_root)

@@ -125,6 +125,21 @@ def test_run_simp_config0_known_answer():
     np.testing.assert_allclose(rpf, g["rho_final"], rtol=1e-10, atol=1e-12)
 
 
+def test_run_simp_heaviside_known_answer():
+    """The projected loop against run_simp with use_heaviside at beta 1 and 8
+    (fixture made by tests/golden/make_golden.py --only heaviside)."""
+    g = load_golden("run_simp_heaviside")
+    nel = (24, 12, 6)
+    bc = fem.cantilever_bc(nel)
+    for beta in (1, 8):
+        rho, hist, cf, rpf = simp.simp_projected(nel, bc, 0.3, 1.5, 3, float(beta), move=0.2)
+        np.testing.assert_allclose(hist, g[f"compliance_b{beta}"], rtol=1e-10)
+        # the bisection stops at a lambda bracket of 1e-9, so the last candidate
+        # carries that much slack; the steep projection (slope up to beta/2)
+        # amplifies it in the physical density
+        np.testing.assert_allclose(rpf, g[f"rho_final_b{beta}"], rtol=1e-9, atol=1e-9)
+
+
 def test_known_answers_from_survey():
     """Self-generated known answers quoted for the config-0 cantilever."""
     nel = (24, 12, 6)

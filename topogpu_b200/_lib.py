@@ -45,6 +45,8 @@ SIGNATURES = {
     "topo_filter": (_i, [_vp, _d, _vp, _vp, _i, _vp]),
     "topo_oc": (_i, [_vp, _vp, _vp, _d, _d, _d, _vp, C.POINTER(_i), _vp]),
     "topo_oc_filtered": (_i, [_vp, _vp, _vp, _vp, _vp, _d, _d, _d, _vp, C.POINTER(_i), _vp]),
+    "topo_heaviside": (_i, [_vp, _vp, _d, _d, _vp, _vp, _vp]),
+    "topo_oc_projected": (_i, [_vp, _d, _vp, _vp, _vp, _d, _d, _d, _d, _d, _vp, C.POINTER(_i), _vp]),
     "topo_oc_noalloc": (_i, [_vp, _vp, _ll, _d, _d, _d, _vp, C.POINTER(_i), _vp]),
     "topo_field_stats": (_i, [_vp, _vp, _ll, C.POINTER(_d), _vp]),
     "topo_gmg_info": (_i, [_vp, C.POINTER(_ll), C.POINTER(_d), C.POINTER(_i)]),

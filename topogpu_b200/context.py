@@ -229,6 +229,32 @@ class TopoContext:
                   "oc_filtered")
         return out, ev.value
 
+    def heaviside(self, rho_f, beta, eta=0.5, phys=None, dh=None, want_deriv=True):
+        """Projection h(rho_f) and, with ``want_deriv``, h'(rho_f)
+        (pub_simp_solver.py:245-253)."""
+        n = self.n_elem
+        phys = torch.empty_like(rho_f) if phys is None else phys
+        if want_deriv and dh is None:
+            dh = torch.empty_like(rho_f)
+        self._chk(self._lib.topo_heaviside(self._h, _ptr(rho_f, torch.float64, n, "rho_f"), float(beta), float(eta),
+                                           _ptr(phys, torch.float64, n, "phys"),
+                                           _ptr(dh, torch.float64, n, "dh") if want_deriv else None, _stream()),
+                  "heaviside")
+        return (phys, dh) if want_deriv else phys
+
+    def oc_projected(self, rmin, rho, dc, dv, beta, eta=0.5, volfrac=0.3, move=0.2, rho_min=1e-3, out=None):
+        """run_simp's OC with the volume measured after filter and projection
+        (pub_simp_solver.py:319-340)."""
+        out = torch.empty_like(rho) if out is None else out
+        ev = C.c_int(0)
+        n = self.n_elem
+        self._chk(self._lib.topo_oc_projected(self._h, float(rmin), _ptr(rho, torch.float64, n, "rho"),
+                                              _ptr(dc, torch.float64, n, "dc"), _ptr(dv, torch.float64, n, "dv"),
+                                              float(beta), float(eta), float(volfrac), float(move), float(rho_min),
+                                              _ptr(out, torch.float64, n, "out"), C.byref(ev), _stream()),
+                  "oc_projected")
+        return out, ev.value
+
     def field_stats(self, x):
         out = (C.c_double * 4)()
         self._chk(self._lib.topo_field_stats(self._h, _ptr(x, torch.float64, None, "x"), x.numel(), out, _stream()),

@@ -1448,6 +1448,37 @@ int topo_oc_filtered(topo_ctx* c, const double* rho, const double* dc, const dou
   }
 }
 
+int topo_heaviside(topo_ctx* c, const double* rho_f, double beta, double eta, double* phys, double* dh,
+                   void* stream) {
+  try {
+    if (!c || !rho_f || (!phys && !dh)) throw std::invalid_argument("topo_heaviside: null pointer");
+    if (phys == rho_f || dh == rho_f) throw std::invalid_argument("topo_heaviside: outputs must not alias rho_f");
+    StreamGuard sg(c, stream);
+    heaviside_apply(c->L[0].g.nelem, rho_f, beta, eta, phys, dh, c->cs);
+    return 0;
+  } catch (const std::exception& e) {
+    return fail(c, e);
+  }
+}
+
+int topo_oc_projected(topo_ctx* c, double rmin, const double* rho, const double* dc, const double* dv, double beta,
+                      double eta, double volfrac, double move, double rho_min, double* out, int* out_evals,
+                      void* stream) {
+  try {
+    if (!c || !rho || !dc || !dv || !out) throw std::invalid_argument("topo_oc_projected: null pointer");
+    if (!(rmin > 0.0)) throw std::invalid_argument("topo_oc_projected: rmin must be > 0");
+    if (out == rho || out == dc || out == dv)
+      throw std::invalid_argument("topo_oc_projected: out must not alias rho, dc or dv");
+    StreamGuard sg(c, stream);
+    const int ev = oc_update_projected(c->L[0].g, rmin, rho, dc, dv, beta, eta, volfrac, move, rho_min, out, c->Hs,
+                                       c->red, c->oc_state, c->cs);
+    if (out_evals) *out_evals = ev;
+    return 0;
+  } catch (const std::exception& e) {
+    return fail(c, e);
+  }
+}
+
 int topo_field_stats(topo_ctx* c, const double* x, long long n, double* out_host, void* stream) {
   try {
     if (!c || !x || !out_host) throw std::invalid_argument("topo_field_stats: null pointer");

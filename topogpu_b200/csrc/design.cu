@@ -271,6 +271,126 @@ int oc_update_filtered(long long n, const double* rho, const double* dc, const d
   return (int)h[OF_EVALS];
 }
 
+// ------------------------------------------------- Heaviside projection
+// Smoothed Heaviside of run_simp (pub_simp_solver.py:245-253):
+//   h(x)  = (tanh(b e) + tanh(b (x - e))) / (tanh(b e) + tanh(b (1 - e)))
+//   h'(x) = b (1 - tanh(b (x - e))^2) / (tanh(b e) + tanh(b (1 - e)))
+// with the identity (h = x, h' = 1) unless b > 1e-6, the guard every run_simp
+// call site applies (pub_simp_solver.py:331,348,366). The two tanh constants
+// are computed on the host and passed in the kernel arguments.
+struct Projection {
+  double beta, eta, tbe, den;
+  bool on;
+};
+
+static Projection make_projection(double beta, double eta) {
+  Projection p{beta, eta, 0.0, 1.0, beta > 1e-6};
+  if (p.on) {
+    p.tbe = std::tanh(beta * eta);
+    p.den = p.tbe + std::tanh(beta * (1.0 - eta));
+  }
+  return p;
+}
+
+__global__ void k_heaviside(long long n, const double* __restrict__ rho_f, Projection p, double* __restrict__ phys,
+                            double* __restrict__ dh) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const double x = rho_f[i];
+    if (!p.on) {
+      if (phys) phys[i] = x;
+      if (dh) dh[i] = 1.0;
+      continue;
+    }
+    const double t = tanh(p.beta * (x - p.eta));
+    if (phys) phys[i] = (p.tbe + t) / p.den;
+    if (dh) dh[i] = p.beta * (1.0 - t * t) / p.den;
+  }
+}
+
+void heaviside_apply(long long n, const double* rho_f, double beta, double eta, double* phys, double* dh,
+                     cudaStream_t s) {
+  const Projection p = make_projection(beta, eta);
+  if (n == 0) return;
+  const unsigned nb = (unsigned)std::min<long long>(4 * kRedBlocks, (n + 255) / 256);
+  k_heaviside<<<nb, 256, 0, s>>>(n, rho_f, p, phys, dh);
+  TOPO_LAUNCH_CHECK();
+}
+
+// ------------------------------------------------- projected-volume OC
+// run_simp's OC with Heaviside (pub_simp_solver.py:319-340): the volume of a
+// candidate is sum_i h((H cand)_i) / n. The projection is nonlinear, so the
+// colsum shortcut of the filtered OC does not apply; each bisection pass
+// writes the candidate (k_ocp_cand) and then filters it at every element,
+// projects and sums in one kernel (k_ocp_vol) whose last block advances the
+// bisection exactly as k_ocf_pass does. The candidate buffer is the output
+// array: once the bisection stops, k_ocp_cand skips, so the output holds the
+// candidate of the last evaluated lambda, which is what the reference returns.
+__global__ void k_ocp_cand(long long n, const double* __restrict__ rho, const double* __restrict__ dc,
+                           const double* __restrict__ dv, double move, double rho_min, const double* st,
+                           double* __restrict__ cand) {
+  if (st[OF_DONE] != 0.0) return;
+  const double lm = st[OF_LM];
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    cand[i] = ocf_candidate(rho[i], dc[i], dv[i], lm, move, rho_min);
+}
+
+__global__ void k_ocp_vol(Grid g, int noff, const double* __restrict__ cand, const double* __restrict__ Hs,
+                          Projection p, double volfrac, double* st, RedWork red) {
+  if (st[OF_DONE] != 0.0) return;
+  const double lm = st[OF_LM];
+  double v[1] = {0.0};
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < g.nelem;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int ez = e % g.nz, ey = (e / g.nz) % g.ny, ex = e / ((long long)g.nz * g.ny);
+    const double hs = Hs[e];
+    double acc = 0.0;
+    for (int k = 0; k < noff; ++k) {
+      const int x = ex + cFoff[k][0], y = ey + cFoff[k][1], z = ez + cFoff[k][2];
+      if (x < 0 || x >= g.nx || y < 0 || y >= g.ny || z < 0 || z >= g.nz) continue;
+      acc += (cFw[k] / hs) * cand[((long long)x * g.ny + y) * g.nz + z];
+    }
+    v[0] += p.on ? (p.tbe + tanh(p.beta * (acc - p.eta))) / p.den : acc;
+  }
+  double tot[1];
+  if (grid_sum<1>(v, red, tot) && threadIdx.x == 0) {
+    st[OF_EVALS] += 1.0;
+    if (tot[0] / (double)g.nelem > volfrac) st[OF_L1] = lm;
+    else st[OF_L2] = lm;
+    st[OF_LAST] = lm;
+    st[OF_K] += 1.0;
+    if (st[OF_L2] - st[OF_L1] < 1e-9 || st[OF_K] >= 100.0) st[OF_DONE] = 1.0;
+    else st[OF_LM] = 0.5 * (st[OF_L1] + st[OF_L2]);
+  }
+}
+
+int oc_update_projected(const Grid& g, double rmin, const double* rho, const double* dc, const double* dv,
+                        double beta, double eta, double volfrac, double move, double rho_min, double* out,
+                        double* Hs_work, RedWork red, double* st, cudaStream_t s) {
+  const long long n = g.nelem;
+  set_filter(rmin, s);
+  const Projection p = make_projection(beta, eta);
+  const unsigned nb = (unsigned)std::min<long long>(kRedBlocks, (n + kRedThreads - 1) / kRedThreads);
+  k_filter_rowsum<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(g, g_filter.n, Hs_work);
+  TOPO_LAUNCH_CHECK();
+  k_ocf_init<<<1, 1, 0, s>>>(st);
+  TOPO_LAUNCH_CHECK();
+  double h[16];
+  int launched = 0;
+  while (true) {
+    for (int k = 0; k < 16 && launched < 100; ++k, ++launched) {
+      k_ocp_cand<<<nb, kRedThreads, 0, s>>>(n, rho, dc, dv, move, rho_min, st, out);
+      TOPO_LAUNCH_CHECK();
+      k_ocp_vol<<<nb, kRedThreads, 0, s>>>(g, g_filter.n, out, Hs_work, p, volfrac, st, red);
+      TOPO_LAUNCH_CHECK();
+    }
+    TOPO_CUDA_CHECK(cudaMemcpyAsync(h, st, sizeof(double) * 16, cudaMemcpyDeviceToHost, s));
+    TOPO_CUDA_CHECK(cudaStreamSynchronize(s));
+    if (h[OF_DONE] != 0.0) break;
+    if (launched >= 100) throw std::runtime_error("projected OC bisection did not terminate");
+  }
+  return (int)h[OF_EVALS];
+}
+
 // ------------------------------------------------------------ field stats
 __global__ void k_stats(long long n, const double* __restrict__ x, double* out4, RedWork red) {
   double sum = 0.0, gray = 0.0, mn = INFINITY, mx = -INFINITY;

@@ -300,6 +300,11 @@ int oc_update(long long n, const double* rho, const double* dc, double volfrac, 
 int oc_update_filtered(long long n, const double* rho, const double* dc, const double* dv,
                        const double* colsum, double volfrac, double move, double rho_min, double* out,
                        RedWork red, double* state, cudaStream_t s);
+void heaviside_apply(long long n, const double* rho_f, double beta, double eta, double* phys, double* dh,
+                     cudaStream_t s);
+int oc_update_projected(const Grid& g, double rmin, const double* rho, const double* dc, const double* dv,
+                        double beta, double eta, double volfrac, double move, double rho_min, double* out,
+                        double* Hs_work, RedWork red, double* st, cudaStream_t s);
 void field_stats(long long n, const double* x, double* out4_dev, RedWork red, cudaStream_t s);
 
 // error plumbing

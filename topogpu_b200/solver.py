@@ -12,6 +12,12 @@ OC on the plain mean volume. ``use_filter=True`` switches to the filtered
 formulation of the reference's CPU driver ``run_simp``
 (src/gpu_fem/pub_simp_solver.py:342-377): physical density H rho,
 sensitivities chained through H^T, volume measured after the filter.
+``use_heaviside=True`` (with ``use_filter``) adds run_simp's smoothed
+Heaviside projection at ``beta``/``eta`` (pub_simp_solver.py:245-253,
+342-377): rho_phys = h(H rho), sensitivities chained through h' and H^T, the
+OC volume measured after filter and projection. ``SIMPLoop.beta`` may be
+changed between steps (run_simp's continuation changes beta the same way,
+between iterations, 379-386).
 """
 
 from __future__ import annotations
@@ -69,13 +75,14 @@ class SIMPSolver:
     Reference arguments: backend, linear_solver, optimizer, tol, max_krylov,
     max_iter, move, rho_min. Extra (optional) arguments: precision
     ("mixed" default, "fp32", "fp64"), levels, fine_degree, coarse_degree,
-    use_filter, penal, smoother ("chebyshev" default, "reference"), device.
+    use_filter, use_heaviside, beta, eta, penal, smoother ("chebyshev"
+    default, "reference"), device.
     """
 
     def __init__(self, backend="cuda", linear_solver="auto", optimizer="oc", tol=1.0e-5, max_krylov=800,
                  max_iter=12, move=0.10, rho_min=1.0e-3, *, precision="mixed", levels=4, fine_degree=2,
-                 coarse_degree=2, use_filter=False, penal=3.0, smoother="chebyshev", coarse_lag=None,
-                 device=None):
+                 coarse_degree=2, use_filter=False, use_heaviside=False, beta=1.0, eta=0.5, penal=3.0,
+                 smoother="chebyshev", coarse_lag=None, device=None):
         if optimizer != "oc":
             raise ValueError("Only optimizer='oc' is implemented in v0.1.0.")
         if backend in {"cpu", "scipy"}:
@@ -92,7 +99,11 @@ class SIMPSolver:
         self.move, self.rho_min = move, rho_min
         self.precision, self.levels = precision, levels
         self.fine_degree, self.coarse_degree = fine_degree, coarse_degree
+        if use_heaviside and not use_filter:
+            raise ValueError("use_heaviside=True needs use_filter=True (run_simp projects the filtered density)")
         self.use_filter = use_filter
+        self.use_heaviside = bool(use_heaviside)
+        self.beta, self.eta = float(beta), float(eta)
         self.penal = penal
         self.smoother = smoother
         # one-setup-lagged coarsest factor built in the background: off by default
@@ -154,13 +165,23 @@ class SIMPLoop:
         self.rho = torch.full((ctx.n_elem,), self.volfrac, dtype=torch.float64, device=dev)
         self.iteration = 0
         self.rmin = None
+        self.beta = solver.beta if solver.use_heaviside else None
+        self.eta = solver.eta
         if solver.use_filter:
             self.rmin = float(problem.filter_radius or spec.rmin or 1.5)
             self.colsum = ctx.filter(self.rmin, torch.ones_like(self.rho), transpose=True)  # H^T 1
 
     def step(self, *, stats: bool = True) -> dict[str, Any]:
         s, ctx = self.solver, self.state.ctx
-        if self.rmin is not None:
+        if self.beta is not None:
+            rho_f = ctx.filter(self.rmin, self.rho)
+            rho_phys, dh = ctx.heaviside(rho_f, self.beta, self.eta)
+            compliance, dc = self.state.solve(rho_phys, s.penal)
+            dc_design = ctx.filter(self.rmin, dc.mul_(dh), transpose=True)
+            dv_design = ctx.filter(self.rmin, dh, transpose=True)
+            self.rho, _ = ctx.oc_projected(self.rmin, self.rho, dc_design, dv_design, self.beta, self.eta,
+                                           self.volfrac, s.move, s.rho_min)
+        elif self.rmin is not None:
             rho_phys = ctx.filter(self.rmin, self.rho)
             compliance, dc = self.state.solve(rho_phys, s.penal)
             dc_design = ctx.filter(self.rmin, dc, transpose=True)
