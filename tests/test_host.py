@@ -58,6 +58,25 @@ def test_generate_bc_matches_reference(tag, nel):
     assert np.array_equal(bc2.F, g[f"side_F_{tag}"])
 
 
+def test_nearest_node_closed_form_matches_bruteforce():
+    """The 8-neighbour nearest-node search picks the node the reference's
+    argmin over all nodes picks, ties (cell midpoints, faces) and points
+    outside the box included."""
+    from topogpu_b200.bc import _nearest, _nearest_bruteforce, node_coords
+    from topogpu_b200.problem_spec import ProblemSpec
+
+    rng = np.random.default_rng(3)
+    for nel, L in [((4, 3, 2), (4.0, 3.0, 2.0)), ((7, 5, 3), (1.0, 0.7, 0.3)), ((10, 4, 6), (2.5, 1.0, 1.5))]:
+        spec = ProblemSpec(nelx=nel[0], nely=nel[1], nelz=nel[2], Lx=L[0], Ly=L[1], Lz=L[2])
+        c = node_coords(spec)
+        h = np.array(L) / np.array(nel)
+        pts = list(rng.uniform(-0.3, 1.3, (200, 3)) * np.array(L))
+        pts += list((rng.integers(0, 2 * np.array(nel) + 1, (200, 3)) * 0.5) * h)  # nodes, midpoints
+        pts += [np.array(L), np.zeros(3), np.array(L) / 2]
+        for p in pts:
+            assert _nearest(spec, c, p) == _nearest_bruteforce(c, p), (nel, p)
+
+
 def test_problem_validation_errors():
     import topogpu_b200 as tg
 

@@ -6,6 +6,12 @@ components of every face node, point supports and point loads snap to the
 nearest node (first index on ties), distributed loads use trapezoidal
 tributary areas, loads on fixed DoFs are zeroed, and an all-zero free load is
 an error. Face node order (and hence F) matches the reference's loops.
+
+Everything is closed form over the structured grid, so the cost is linear in
+the DoF count with no Python loop over nodes: the nearest node is searched
+among the (up to) 8 grid nodes around the point with the same distance
+arithmetic as a search over all nodes, and the free set is the complement of
+a boolean mask (at 8M elements the setup takes a fraction of a second).
 """
 
 from __future__ import annotations
@@ -33,8 +39,11 @@ class BCResult:
 
 def node_coords(spec: ProblemSpec) -> np.ndarray:
     nx, ny, nz = spec.nelx, spec.nely, spec.nelz
-    i, j, k = np.meshgrid(np.arange(nx + 1), np.arange(ny + 1), np.arange(nz + 1), indexing="ij")
-    return np.column_stack([i.ravel() * (spec.Lx / nx), j.ravel() * (spec.Ly / ny), k.ravel() * (spec.Lz / nz)])
+    c = np.empty((nx + 1, ny + 1, nz + 1, 3))
+    c[..., 0] = (np.arange(nx + 1) * (spec.Lx / nx))[:, None, None]
+    c[..., 1] = (np.arange(ny + 1) * (spec.Ly / ny))[None, :, None]
+    c[..., 2] = (np.arange(nz + 1) * (spec.Lz / nz))[None, None, :]
+    return c.reshape(-1, 3)
 
 
 def face_nodes(face: str, nel) -> np.ndarray:
@@ -53,8 +62,28 @@ def face_nodes(face: str, nel) -> np.ndarray:
     raise ValueError(f"Unknown 3D face: {face}")
 
 
-def _nearest(coords: np.ndarray, p) -> int:
+def _nearest_bruteforce(coords: np.ndarray, p) -> int:
+    """Reference rule: argmin of the Euclidean distance over all nodes, the
+    first node on ties (bc_generator.py:108-111)."""
     return int(np.argmin(np.linalg.norm(coords - np.asarray(p, dtype=float)[None, :], axis=1)))
+
+
+def _nearest(spec: ProblemSpec, coords: np.ndarray, p) -> int:
+    """Same node as ``_nearest_bruteforce``: the nearest grid node is one of
+    the 8 nodes of the cell around p (clamped to the grid), and those are
+    compared with the same distance arithmetic, in increasing node order, so
+    ties resolve to the first node as argmin does."""
+    n = (spec.nelx, spec.nely, spec.nelz)
+    L = (spec.Lx, spec.Ly, spec.Lz)
+    p = np.asarray(p, dtype=float)
+    cand = []
+    for ax in range(3):
+        h = L[ax] / n[ax]
+        f = int(np.floor(p[ax] / h)) if np.isfinite(p[ax]) else 0
+        cand.append(sorted({min(max(f + d, 0), n[ax]) for d in (-1, 0, 1, 2)}))
+    ny1, nz1 = n[1] + 1, n[2] + 1
+    ids = np.array(sorted((i * ny1 + j) * nz1 + k for i in cand[0] for j in cand[1] for k in cand[2]))
+    return int(ids[np.argmin(np.linalg.norm(coords[ids] - p[None, :], axis=1))])
 
 
 def _tributary(spec: ProblemSpec, face: str, xyz: np.ndarray) -> np.ndarray:
@@ -82,19 +111,21 @@ def generate_bc(spec: ProblemSpec) -> BCResult:
     nel = (spec.nelx, spec.nely, spec.nelz)
     coords = node_coords(spec)
     ndof = 3 * len(coords)
-    fixed = set()
+    fixed_parts = []
     for sup in spec.supports:
-        nodes = face_nodes(sup.edge, nel) if isinstance(sup, EdgeSupport) else [
-            _nearest(coords, (sup.x, sup.y, sup.z))]
-        for n in nodes:
-            for off in sup.dof_mask(3):
-                fixed.add(3 * int(n) + off)
-    fixed = np.sort(np.fromiter(fixed, dtype=np.int64)) if fixed else np.zeros(0, dtype=np.int64)
-    free = np.setdiff1d(np.arange(ndof), fixed)
+        nodes = face_nodes(sup.edge, nel) if isinstance(sup, EdgeSupport) else np.array(
+            [_nearest(spec, coords, (sup.x, sup.y, sup.z))])
+        offs = np.asarray(list(sup.dof_mask(3)), dtype=np.int64)
+        if offs.size:
+            fixed_parts.append((3 * np.asarray(nodes, dtype=np.int64)[:, None] + offs[None, :]).ravel())
+    fixed = np.unique(np.concatenate(fixed_parts)) if fixed_parts else np.zeros(0, dtype=np.int64)
+    is_free = np.ones(ndof, dtype=bool)
+    is_free[fixed] = False
+    free = np.flatnonzero(is_free).astype(np.int64)
     F = np.zeros(ndof)
     for ld in spec.loads:
         if isinstance(ld, PointLoad):
-            n = _nearest(coords, (ld.x, ld.y, ld.z))
+            n = _nearest(spec, coords, (ld.x, ld.y, ld.z))
             F[3 * n] += ld.fx
             F[3 * n + 1] += ld.fy
             F[3 * n + 2] += ld.fz
@@ -103,8 +134,8 @@ def generate_bc(spec: ProblemSpec) -> BCResult:
             w = _tributary(spec, ld.edge, coords[nodes])
             comp, sign = {"left": (0, -1.0), "right": (0, 1.0), "bottom": (1, -1.0), "top": (1, 1.0),
                           "front": (2, -1.0), "back": (2, 1.0)}[ld.edge]
-            for i, n in enumerate(nodes):
-                F[3 * n + comp] += ld.magnitude * sign * w[i]
+            # face nodes are distinct, so the scatter-add has no repeated index
+            F[3 * nodes + comp] += ld.magnitude * sign * w
     F[fixed] = 0.0
     if np.max(np.abs(F[free])) < 1e-30:
         raise ValueError("Force vector is zero on all free DOFs. "
