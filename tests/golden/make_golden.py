@@ -23,9 +23,11 @@ reference. Every array is produced by reference code paths:
   run_simp.npz     run_simp config 0 (rmin 1.5, move 0.2, no Heaviside)
   run_simp_heaviside.npz  run_simp on the same mesh with Heaviside
                    projection at beta 1 (the SIMPParams default) and beta 8
+  ckpt_24x12x6_cantilever.{npz,json}  the checkpoint run_simp writes after
+                   iteration 2 of config 0 (checkpoint_every 1)
 
-``python make_golden.py [REF_ROOT] [--only heaviside]`` regenerates all
-fixtures, or only the Heaviside ones.
+``python make_golden.py [REF_ROOT] [--only heaviside|checkpoint]``
+regenerates all fixtures, or only the Heaviside or checkpoint ones.
 """
 
 from __future__ import annotations
@@ -223,7 +225,26 @@ def main(ref_root: str) -> None:
     np.savez_compressed(HERE / "run_simp.npz", compliance=np.array(res["compliance_history"]),
                         final=np.array(res["final_compliance"]), rho_final=res["rho_final"])
     heaviside_fixtures(ref_root)
+    checkpoint_fixtures(ref_root)
     print("golden fixtures written to", HERE)
+
+
+def checkpoint_fixtures(ref_root) -> None:
+    import shutil
+    import tempfile
+
+    _setup(Path(ref_root))
+    from gpu_fem.pub_simp_solver import SIMPParams, run_simp
+
+    nel = (24, 12, 6)
+    fixed, free, F, ndof = cantilever_bc(nel)
+    with tempfile.TemporaryDirectory() as d:
+        params = SIMPParams(nelx=24, nely=12, nelz=6, volfrac=0.3, rmin=1.5, move=0.2, max_iter=2, min_iter=2,
+                            use_heaviside=False, checkpoint_dir=d, checkpoint_every=1)
+        with redirect_stdout(io.StringIO()):
+            run_simp(params, verbose=False, bc_override=lambda a, b, c: (fixed, free, F))
+        for ext in (".npz", ".json"):
+            shutil.copy(Path(d) / f"ckpt_24x12x6_cantilever{ext}", HERE / f"ckpt_24x12x6_cantilever{ext}")
 
 
 def heaviside_fixtures(ref_root) -> None:
@@ -249,9 +270,11 @@ if __name__ == "__main__":
 
     ap = argparse.ArgumentParser()
     ap.add_argument("ref_root", nargs="?", default="/root/reference")
-    ap.add_argument("--only", choices=["heaviside"], default=None)
+    ap.add_argument("--only", choices=["heaviside", "checkpoint"], default=None)
     a = ap.parse_args()
     if a.only == "heaviside":
         heaviside_fixtures(a.ref_root)
+    elif a.only == "checkpoint":
+        checkpoint_fixtures(a.ref_root)
     else:
         main(a.ref_root)

@@ -130,3 +130,41 @@ def test_simp_heaviside_loop_matches_oracle_with_beta_change(cuda_dev):
         rho, _ = design.oc_update_projected(rho, H.T @ (dcp * dh), H.T @ dh, 0.3, 0.2, H, beta, 0.5)
     np.testing.assert_allclose(comp, ref, rtol=1e-8)
     np.testing.assert_allclose(rho_gpu, rho, rtol=1e-6, atol=1e-8)
+
+
+def test_resume_from_reference_checkpoint(cuda_dev, tmp_path):
+    """Resume the filtered SIMP loop from the checkpoint run_simp wrote after
+    iteration 2 of config 0: iteration 3 gives run_simp's third compliance,
+    and the checkpoint written after it carries the whole history."""
+    import shutil
+
+    import topogpu_b200 as tg
+    from conftest import GOLDEN
+    from topogpu_b200.checkpoint import load_checkpoint
+
+    for ext in (".npz", ".json"):
+        shutil.copy(GOLDEN / f"ckpt_24x12x6_cantilever{ext}", tmp_path / f"ckpt_24x12x6_cantilever{ext}")
+    g = load_golden("run_simp")
+    p = tg.gallery.benchmark_cantilever((24, 12, 6), volfrac=0.3, filter_radius=1.5)
+    res = tg.SIMPSolver(backend="cuda", tol=1e-10, max_krylov=800, max_iter=3, move=0.2, precision="fp64",
+                        use_filter=True, checkpoint_dir=str(tmp_path), checkpoint_every=1).solve(p)
+    assert [r["iteration"] for r in res.history] == [3]
+    np.testing.assert_allclose(res.history[0]["compliance"], g["compliance"][2], rtol=1e-8)
+    ck = load_checkpoint(str(tmp_path / "ckpt_24x12x6_cantilever"))
+    assert ck["iteration"] == 3
+    np.testing.assert_allclose(ck["compliance_hist"], g["compliance"], rtol=1e-8)
+
+
+def test_interrupted_run_resumes_to_same_history(cuda_dev, tmp_path):
+    """Two iterations, a checkpoint, then a fresh solver resuming to four
+    iterations gives the compliances of one uninterrupted four-iteration run."""
+    import topogpu_b200 as tg
+
+    p = tg.gallery.benchmark_cantilever((24, 12, 6), volfrac=0.3, filter_radius=1.5)
+    kw = dict(backend="cuda", tol=1e-10, max_krylov=800, move=0.2, precision="fp64", use_filter=True,
+              use_heaviside=True, beta=2.0)
+    full = [r["compliance"] for r in tg.SIMPSolver(max_iter=4, **kw).solve(p).history]
+    tg.SIMPSolver(max_iter=2, checkpoint_dir=str(tmp_path), checkpoint_every=2, **kw).solve(p)
+    rest = tg.SIMPSolver(max_iter=4, checkpoint_dir=str(tmp_path), checkpoint_every=2, **kw).solve(p)
+    assert [r["iteration"] for r in rest.history] == [3, 4]
+    np.testing.assert_allclose([r["compliance"] for r in rest.history], full[2:], rtol=1e-7)

@@ -158,3 +158,36 @@ def test_autograd_compliance_plumbing_without_gpu():
     (2.0 * c).backward()
     assert torch.allclose(rho.grad, 6.0 * rho.detach() ** 2)
     assert abs(float(c) - float((rho.detach() ** 3).sum())) < 1e-12
+
+
+def test_checkpoint_format_matches_reference(tmp_path):
+    """A run_simp checkpoint (written by the reference after iteration 2 of
+    config 0) loads here with every key, and writing it back gives files the
+    reference's loader reads to the same values (pub_simp_solver.py:397-410)."""
+    import json
+    import shutil
+
+    from conftest import GOLDEN
+    from topogpu_b200.checkpoint import ARRAY_KEYS, SCALAR_KEYS, checkpoint_path, load_checkpoint, save_checkpoint
+
+    assert checkpoint_path(str(tmp_path), (24, 12, 6)) == str(tmp_path / "ckpt_24x12x6_cantilever")
+    src = str(GOLDEN / "ckpt_24x12x6_cantilever")
+    ck = load_checkpoint(src)
+    assert set(ck) == set(ARRAY_KEYS) | set(SCALAR_KEYS)
+    assert ck["iteration"] == 2 and ck["best_compliance"] == float("inf") and ck["best_is_valid"] == 0
+    assert ck["rho"].shape == (1728,) and len(ck["compliance_hist"]) == 2
+    out = str(tmp_path / "ckpt_24x12x6_cantilever")
+    save_checkpoint(out, {k: ck[k] for k in ck})
+    back = load_checkpoint(out)
+    for k in ARRAY_KEYS:
+        assert np.array_equal(back[k], ck[k]), k
+    for k in SCALAR_KEYS:
+        assert back[k] == ck[k], k
+    with open(out + ".json") as f, open(src + ".json") as g:
+        assert json.load(f) == json.load(g)
+    with np.load(out + ".npz") as a, np.load(src + ".npz") as b:
+        assert sorted(a.files) == sorted(b.files)
+    assert not (tmp_path / "ckpt_24x12x6_cantilever.tmp.npz").exists()
+    # a missing half means no checkpoint, as in the reference
+    shutil.copy(src + ".npz", tmp_path / "only.npz")
+    assert load_checkpoint(str(tmp_path / "only")) is None
