@@ -73,6 +73,12 @@ int topo_ctx_destroy(topo_ctx* ctx);
  * by the level's FP32 (or FP64) operator. */
 int topo_set_smoother(topo_ctx* ctx, int form, double lam_safety);
 
+/* Multigrid cycle: gamma 1 = V-cycle (default; multigrid_v4.py:986-1008),
+ * gamma 2 = W-cycle, two coarse corrections per level (multigrid_v4.py:
+ * 1010-1042, GalerkinMatFreeGMG(cycle_type="w"), SolverV4(gmg_cycle_type)).
+ * Takes effect at the next preconditioner application. */
+int topo_set_cycle(topo_ctx* ctx, int gamma);
+
 /* Copy the last error message of this context (or of the library, if ctx is
  * NULL) into buf. Returns the message length. */
 int topo_last_error(topo_ctx* ctx, char* buf, int len);

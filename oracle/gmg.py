@@ -228,7 +228,10 @@ class GMG:
 
     def __init__(self, nel, free, n_levels=4, fine_prec="fp64", fine_degree=2, coarse_iters=2,
                  cheb_lower_frac=1.0 / 30.0, dense_chol_max=5000, coarse_pcg_iters=80,
-                 level_prec=None):
+                 level_prec=None, cycle="v"):
+        if cycle not in ("v", "w"):
+            raise ValueError("cycle must be 'v' or 'w'")
+        self.cycle = cycle
         self.nel = tuple(nel)
         self.n_levels = n_levels
         self.fine_prec = fine_prec
@@ -350,5 +353,20 @@ class GMG:
         x = x + self.P[lv] @ ec
         return self.smooth_fine(x, rhs) if lv == 0 else self.smooth_coarse(lv, x, rhs)
 
+    def wcycle(self, lv, rhs):
+        """multigrid_v4.py:1010-1042: two coarse corrections per level, the
+        second on the residual after the first."""
+        if lv == self.n_levels - 1:
+            if self.n_levels == 1:
+                return self.smooth_fine(np.zeros_like(rhs), rhs, True)
+            return self.solve_coarsest(rhs)
+        z = np.zeros_like(rhs)
+        op = self.fine_op64 if lv == 0 else (lambda v: self.K[lv] @ v)
+        x = self.smooth_fine(z, rhs, True) if lv == 0 else self.smooth_coarse(lv, z, rhs, True)
+        x = x + self.P[lv] @ self.wcycle(lv + 1, self.P[lv].T @ (rhs - op(x)))
+        x = x + self.P[lv] @ self.wcycle(lv + 1, self.P[lv].T @ (rhs - op(x)))
+        return self.smooth_fine(x, rhs) if lv == 0 else self.smooth_coarse(lv, x, rhs)
+
     def apply(self, r):
-        return self.vcycle(0, np.asarray(r, dtype=np.float64))
+        r = np.asarray(r, dtype=np.float64)
+        return self.wcycle(0, r) if self.cycle == "w" else self.vcycle(0, r)

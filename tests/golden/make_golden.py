@@ -23,11 +23,13 @@ reference. Every array is produced by reference code paths:
   run_simp.npz     run_simp config 0 (rmin 1.5, move 0.2, no Heaviside)
   run_simp_heaviside.npz  run_simp on the same mesh with Heaviside
                    projection at beta 1 (the SIMPParams default) and beta 8
+  wcycle.npz       GalerkinMatFreeGMG(cycle_type="w").apply and PCG on the
+                   galerkin.npz hierarchies
   ckpt_24x12x6_cantilever.{npz,json}  the checkpoint run_simp writes after
                    iteration 2 of config 0 (checkpoint_every 1)
 
-``python make_golden.py [REF_ROOT] [--only heaviside|checkpoint]``
-regenerates all fixtures, or only the Heaviside or checkpoint ones.
+``python make_golden.py [REF_ROOT] [--only heaviside|checkpoint|wcycle]``
+regenerates all fixtures, or only the named group.
 """
 
 from __future__ import annotations
@@ -226,7 +228,41 @@ def main(ref_root: str) -> None:
                         final=np.array(res["final_compliance"]), rho_final=res["rho_final"])
     heaviside_fixtures(ref_root)
     checkpoint_fixtures(ref_root)
+    wcycle_fixtures(ref_root)
     print("golden fixtures written to", HERE)
+
+
+def wcycle_fixtures(ref_root) -> None:
+    _setup(Path(ref_root))
+    import cupy as cp
+    import gpu_fem.multigrid_v4 as mg
+    import gpu_fem.solver_v2 as sv2
+    from gpu_fem.pub_simp_solver import KE_UNIT_3D, _edof_table_3d
+
+    d = {}
+    for nel, nlev in [((24, 12, 6), 4), ((7, 5, 3), 3)]:
+        tag = "x".join(map(str, nel))
+        edof = _edof_table_3d(*nel)
+        fixed, free, F, ndof = cantilever_bc(nel)
+        rng = np.random.default_rng(11)
+        rho = rng.uniform(0.05, 1.0, edof.shape[0])  # the galerkin.npz density
+        E = 1e-9 + (1 - 1e-9) * rho**3
+        free_gpu = cp.asarray(free.astype(np.int32))
+        op = sv2.MatrixFreeKff(cp.asarray(edof), cp.asarray(KE_UNIT_3D), free_gpu, len(free), ndof)
+        with redirect_stdout(io.StringIO()):
+            g = mg.GalerkinMatFreeGMG(mf_op=op, free=free.astype(np.int32), free_gpu=free_gpu, nelx=nel[0],
+                                      nely=nel[1], nelz=nel[2], KE_UNIT=KE_UNIT_3D, n_levels=nlev,
+                                      fine_smoother="fp64", fine_smoother_degree=2, cycle_type="w")
+            g.setup(cp.asarray(E))
+        r = np.random.default_rng(12).standard_normal(len(free))
+        d[f"rho_{tag}"] = rho
+        d[f"r_{tag}"] = r
+        d[f"z_{tag}"] = np.asarray(g.apply(cp.asarray(r)))
+        Fd = cp.asarray(F[free])
+        x, it, ok = sv2._cupy_pcg(lambda v: op.matvec(v, cp.asarray(E)), Fd, g.apply, tol=1e-8, maxiter=500)
+        d[f"pcg_x_{tag}"] = np.asarray(x)
+        d[f"pcg_it_{tag}"] = np.array(it)
+    np.savez_compressed(HERE / "wcycle.npz", **d)
 
 
 def checkpoint_fixtures(ref_root) -> None:
@@ -270,11 +306,13 @@ if __name__ == "__main__":
 
     ap = argparse.ArgumentParser()
     ap.add_argument("ref_root", nargs="?", default="/root/reference")
-    ap.add_argument("--only", choices=["heaviside", "checkpoint"], default=None)
+    ap.add_argument("--only", choices=["heaviside", "checkpoint", "wcycle"], default=None)
     a = ap.parse_args()
     if a.only == "heaviside":
         heaviside_fixtures(a.ref_root)
     elif a.only == "checkpoint":
         checkpoint_fixtures(a.ref_root)
+    elif a.only == "wcycle":
+        wcycle_fixtures(a.ref_root)
     else:
         main(a.ref_root)

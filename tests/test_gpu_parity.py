@@ -226,6 +226,55 @@ def test_pcg_and_fgmres_fp64_match_reference(cuda_dev, tag, nel, nlev):
     assert _rel(x2.cpu().numpy()[bc.free], g[f"fgmres_x_{tag}"]) < 1e-9
 
 
+@pytest.mark.parametrize("tag,nel,nlev", [("24x12x6", (24, 12, 6), 4), ("7x5x3", (7, 5, 3), 3)])
+def test_wcycle_fp64_matches_reference(cuda_dev, tag, nel, nlev):
+    """W-cycle (two coarse corrections per level, multigrid_v4.py:1010-1042)
+    against GalerkinMatFreeGMG(cycle_type="w"): one application to 1e-10, and
+    PCG on it. PCG with this W-cycle is sensitive to rounding (1e-14 noise in
+    F moves the reference count over 39-41 and 141-162), so the count is held
+    to a 15% band and the solution to 1e-6."""
+    g = load_golden("wcycle")
+    ctx, bc, _ = _ctx(nel, n_levels=nlev)
+    ctx.set_cycle("w")
+    ctx.gmg_setup(_t(fem.simp_modulus(g[f"rho_{tag}"])))
+    r = np.zeros(bc.ndof)
+    r[bc.free] = g[f"r_{tag}"]
+    z = ctx.gmg_apply(_t(r)).cpu().numpy()
+    assert _rel(z[bc.free], g[f"z_{tag}"]) < 1e-10
+    x = torch.zeros(bc.ndof, dtype=torch.float64, device=DEV)
+    it, rr, ok = ctx.pcg(_t(bc.F), x, tol=1e-8, maxiter=500)
+    ref_it = int(g[f"pcg_it_{tag}"])
+    assert ok and rr < 1e-8 and abs(it - ref_it) <= max(2, 0.15 * ref_it)
+    assert _rel(x.cpu().numpy()[bc.free], g[f"pcg_x_{tag}"]) < 1e-6
+    ctx.set_cycle("v")  # back to the V-cycle: the galerkin.npz application again
+    zv = ctx.gmg_apply(_t(r)).cpu().numpy()
+    gv = load_golden("galerkin")
+    rv = np.zeros(bc.ndof)
+    rv[bc.free] = gv[f"r_{tag}"]
+    assert _rel(ctx.gmg_apply(_t(rv)).cpu().numpy()[bc.free], gv[f"z_{tag}"]) < 1e-10
+    assert not np.allclose(zv, z)
+
+
+def test_wcycle_mixed_chebyshev_converges(cuda_dev):
+    """The W-cycle with the default Chebyshev smoother and the mixed
+    schedule solves to tolerance in no more iterations than the V-cycle."""
+    from topogpu_b200.bc import cantilever_edge_load
+    from topogpu_b200.state import StateSolver
+
+    nel = (32, 16, 16)
+    free, F = cantilever_edge_load(nel)
+    rho = torch.as_tensor(np.random.default_rng(3).uniform(0.05, 1.0, int(np.prod(nel))), device=DEV)
+    its = {}
+    for cyc in ("v", "w"):
+        st = StateSolver(nel, free, F, n_levels=3, precision="mixed", tol=1e-6, cycle_type=cyc)
+        c, _ = st.solve(rho)
+        assert st.last_converged
+        its[cyc] = (st.last_cg_iters, float(c))
+        st.close()
+    assert its["w"][0] <= its["v"][0] + 2
+    assert abs(its["w"][1] - its["v"][1]) < 1e-5 * abs(its["v"][1])
+
+
 def test_pcg_warm_start_converged_up_front(cuda_dev):
     nel = (12, 6, 6)
     ctx, bc, _ = _ctx(nel, n_levels=3)

@@ -125,6 +125,26 @@ def test_run_simp_config0_known_answer():
     np.testing.assert_allclose(rpf, g["rho_final"], rtol=1e-10, atol=1e-12)
 
 
+@pytest.mark.parametrize("tag,nel,nlev", [("24x12x6", (24, 12, 6), 4), ("7x5x3", (7, 5, 3), 3)])
+def test_wcycle_against_reference(tag, nel, nlev):
+    """GalerkinMatFreeGMG(cycle_type="w") on the galerkin.npz hierarchies
+    (multigrid_v4.py:1010-1042): one application and PCG to 1e-8."""
+    g = load_golden("wcycle")
+    bc = fem.cantilever_bc(nel)
+    h = gmg.GMG(nel, bc.free, n_levels=nlev, fine_prec="fp64", fine_degree=2, cycle="w").setup(
+        fem.simp_modulus(g[f"rho_{tag}"]))
+    z = h.apply(g[f"r_{tag}"])
+    assert np.linalg.norm(z - g[f"z_{tag}"]) / np.linalg.norm(g[f"z_{tag}"]) < 1e-10
+    # PCG with this W-cycle is sensitive to rounding: 1e-14 relative noise in
+    # F moves the count over 39-41 (24x12x6) and 141-162 (7x5x3), so the count
+    # is held to a 15% band and the solution to the tolerance
+    x, it, ok = krylov.pcg(h.fine_op64, bc.F[bc.free], h.apply, tol=1e-8, maxiter=500)
+    ref_it = int(g[f"pcg_it_{tag}"])
+    assert ok and abs(it - ref_it) <= max(2, 0.15 * ref_it)
+    xr = g[f"pcg_x_{tag}"]
+    assert np.linalg.norm(x - xr) / np.linalg.norm(xr) < 1e-6
+
+
 def test_run_simp_heaviside_known_answer():
     """The projected loop against run_simp with use_heaviside at beta 1 and 8
     (fixture made by tests/golden/make_golden.py --only heaviside)."""

@@ -38,6 +38,7 @@ SIGNATURES = {
     "topo_fgmres": (_i, [_vp, _vp, _vp, _d, _i, _i, C.POINTER(_i), C.POINTER(_d), _vp]),
     "topo_set_coarse_lag": (_i, [_vp, _i]),
     "topo_set_tc": (_i, [_vp, _i]),
+    "topo_set_cycle": (_i, [_vp, _i]),
     "topo_block_pcg": (_i, [_vp, _vp, _vp, _i, _d, _i, C.POINTER(_i), C.POINTER(_d), _vp]),
     "topo_sensitivity": (_i, [_vp, _vp, _i, _vp, _d, _d, _d, _vp, _vp]),
     "topo_sensitivity_adjoint": (_i, [_vp, _vp, _vp, _i, _vp, _d, _d, _d, _vp, _vp]),

@@ -152,6 +152,13 @@ class TopoContext:
         in the background (see topo_set_coarse_lag)."""
         self._chk(self._lib.topo_set_coarse_lag(self._h, int(bool(on))), "set_coarse_lag")
 
+    def set_cycle(self, cycle_type: str):
+        """"v" (one coarse correction per level) or "w" (two)
+        (multigrid_v4.py:986-1042)."""
+        if cycle_type not in ("v", "w"):
+            raise ValueError(f"cycle_type must be 'v' or 'w'; got {cycle_type!r}")
+        self._chk(self._lib.topo_set_cycle(self._h, 1 if cycle_type == "v" else 2), "set_cycle")
+
     def set_tensor_cores(self, on: bool):
         """BF16 level-0 K.u on tcgen05 (True) or on the CUDA cores (False)."""
         self._chk(self._lib.topo_set_tc(self._h, int(bool(on))), "set_tc")

@@ -177,6 +177,7 @@ struct topo_ctx {
   double lam_safety = 1.25;   // factor on the power-iteration lambda_max
   int dense_max = 16384;
   bool use_tc = true;         // BF16 level-0 operator on tcgen05 (TOPO_B200_NO_TC=1: CUDA cores)
+  int cycle_gamma = 1;        // coarse corrections per level: 1 V-cycle, 2 W-cycle
   bool coarse_lag = false;    // V-cycle uses the previous setup's coarsest factor; the new one builds in the background
   std::vector<Level> L;
   Coarsest C;
@@ -320,7 +321,11 @@ void coarsest_solve(topo_ctx* c, const KrylovState* st, cudaStream_t s) {
   dense_apply(c->vec64, c->C.n, c->C.ldc, c->C.cur.work, c->C.cur.X32, c->C.free_list, Lv.b, c->C.y, Lv.x, st, s);
 }
 
-// One V-cycle on level l (multigrid_v4.py:986-1008): input Lv.b, output Lv.x.
+// One V-cycle (cycle_gamma 1, multigrid_v4.py:986-1008) or W-cycle
+// (cycle_gamma 2, multigrid_v4.py:1010-1042) on level l: input Lv.b, output
+// Lv.x. Each coarse correction restricts the recursive residual, recurses,
+// adds e = P x_c and updates r -= K e, so the second correction of a W-cycle
+// restricts b - K x without a separate residual product.
 void vcycle(topo_ctx* c, int l, const KrylovState* st, cudaStream_t s) {
   Level& Lv = c->L[l];
   if (l == c->n_levels - 1) {
@@ -330,14 +335,16 @@ void vcycle(topo_ctx* c, int l, const KrylovState* st, cudaStream_t s) {
   }
   smooth(c, l, true, true, st, s);  // x = S b, r = b - K x
   Level& Lc = c->L[l + 1];
-  restrict_vec(c->vec64, Lv.g, Lc.g, Lv.r, Lc.mask, Lc.b, st, s);
-  vcycle(c, l + 1, st, s);
-  prolong_add(c->vec64, Lv.g, Lc.g, Lc.x, Lv.mask, Lv.x, Lv.e, st, s);  // x += e = P x_c
-  EpiArgs ea{};
-  ea.r = Lv.r;
-  ea.s = 1.0;
-  ea.st = const_cast<KrylovState*>(st);
-  op_apply(c, l, hi_prec(Lv), Lv.e, nullptr, Epi::RUpd, ea, s);  // r -= K e
+  for (int k = 0; k < c->cycle_gamma; ++k) {
+    restrict_vec(c->vec64, Lv.g, Lc.g, Lv.r, Lc.mask, Lc.b, st, s);
+    vcycle(c, l + 1, st, s);
+    prolong_add(c->vec64, Lv.g, Lc.g, Lc.x, Lv.mask, Lv.x, Lv.e, st, s);  // x += e = P x_c
+    EpiArgs ea{};
+    ea.r = Lv.r;
+    ea.s = 1.0;
+    ea.st = const_cast<KrylovState*>(st);
+    op_apply(c, l, hi_prec(Lv), Lv.e, nullptr, Epi::RUpd, ea, s);  // r -= K e
+  }
   smooth(c, l, false, false, st, s);
 }
 
@@ -634,6 +641,7 @@ void pcg_iteration(topo_ctx* c, cudaStream_t s) {
 
 std::vector<double> pcg_graph_key(const topo_ctx* c) {
   std::vector<double> k = {(double)c->cheb_form, c->lam_safety, c->cheb_lower, (double)c->use_tc,
+                           (double)c->cycle_gamma,
                            (double)c->fine_degree, (double)c->coarse_degree,
                            (double)reinterpret_cast<uintptr_t>(c->C.cur.work), (double)reinterpret_cast<uintptr_t>(c->C.cur.X32),
                            (double)reinterpret_cast<uintptr_t>(c->C.y), (double)c->C.n, (double)c->C.ldc};
@@ -1340,6 +1348,17 @@ int topo_set_coarse_lag(topo_ctx* c, int on) {
   try {
     if (!c) throw std::invalid_argument("topo_set_coarse_lag: null context");
     c->coarse_lag = on != 0;
+    return 0;
+  } catch (const std::exception& e) {
+    return fail(c, e);
+  }
+}
+
+int topo_set_cycle(topo_ctx* c, int gamma) {
+  try {
+    if (!c) throw std::invalid_argument("topo_set_cycle: null context");
+    if (gamma != 1 && gamma != 2) throw std::invalid_argument("topo_set_cycle: gamma must be 1 (V) or 2 (W)");
+    c->cycle_gamma = gamma;
     return 0;
   } catch (const std::exception& e) {
     return fail(c, e);

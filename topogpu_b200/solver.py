@@ -80,14 +80,15 @@ class SIMPSolver:
     use_filter, use_heaviside, beta, eta, penal, smoother ("chebyshev"
     default, "reference"), checkpoint_dir / checkpoint_every /
     checkpoint_problem (run_simp's checkpoint files: resume from one when it
-    exists, write one every checkpoint_every iterations), device.
+    exists, write one every checkpoint_every iterations), cycle_type ("v"
+    default, "w": SolverV4's gmg_cycle_type), device.
     """
 
     def __init__(self, backend="cuda", linear_solver="auto", optimizer="oc", tol=1.0e-5, max_krylov=800,
                  max_iter=12, move=0.10, rho_min=1.0e-3, *, precision="mixed", levels=4, fine_degree=2,
                  coarse_degree=2, use_filter=False, use_heaviside=False, beta=1.0, eta=0.5, penal=3.0,
                  smoother="chebyshev", coarse_lag=None, checkpoint_dir=None, checkpoint_every=10,
-                 checkpoint_problem="cantilever", device=None):
+                 checkpoint_problem="cantilever", cycle_type="v", device=None):
         if optimizer != "oc":
             raise ValueError("Only optimizer='oc' is implemented in v0.1.0.")
         if backend in {"cpu", "scipy"}:
@@ -119,6 +120,9 @@ class SIMPSolver:
             raise ValueError("checkpoint_every must be >= 1")
         self.checkpoint_dir, self.checkpoint_every = checkpoint_dir, int(checkpoint_every)
         self.checkpoint_problem = checkpoint_problem
+        if cycle_type not in ("v", "w"):
+            raise ValueError(f"cycle_type must be 'v' or 'w'; got {cycle_type!r}")
+        self.cycle_type = cycle_type
         self.device = device
 
     def make_state_solver(self, problem: TopologyProblem) -> StateSolver:
@@ -130,7 +134,8 @@ class SIMPSolver:
         outer = "fgmres" if self.linear_solver == "fgmres_gmg" else "pcg"
         st = StateSolver(problem.nel, bc.free_mask(), F, n_levels=self.levels, precision=self.precision,
                          fine_degree=self.fine_degree, coarse_degree=self.coarse_degree, outer=outer,
-                         tol=self.tol, maxiter=self.max_krylov, smoother=self.smoother, device=self.device)
+                         tol=self.tol, maxiter=self.max_krylov, smoother=self.smoother, cycle_type=self.cycle_type,
+                         device=self.device)
         st.ctx.set_coarse_lag(self.coarse_lag)
         return st
 
