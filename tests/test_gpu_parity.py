@@ -162,6 +162,27 @@ def test_vcycle_fp64_matches_reference(cuda_dev, tag, nel, nlev):
         assert info["n_free"][lv] == len(g[f"free{lv}_{tag}"])
 
 
+@pytest.mark.parametrize("nel,nlev", [((24, 12, 6), 2), ((32, 16, 16), 2)])
+def test_multi_panel_coarsest_factor_matches_oracle(cuda_dev, nel, nlev):
+    """A coarsest system of many 32-column panels (1,008 and 3,888 free DoFs)
+    factorised and inverted on the device: the
+    V-cycle against the oracle's, whose coarsest solve is scipy's dense
+    Cholesky (dense_chol_max raised to cover it)."""
+    bc = fem.cantilever_bc(nel)
+    rho = np.random.default_rng(9).uniform(0.05, 1.0, int(np.prod(nel)))
+    E = fem.simp_modulus(rho)
+    h = gmg.GMG(nel, bc.free, n_levels=nlev, fine_prec="fp64", fine_degree=2, dense_chol_max=20000).setup(E)
+    assert h.chol is not None
+    ctx, _, _ = _ctx(nel, n_levels=nlev, bc=bc)
+    ctx.gmg_setup(_t(E))
+    assert ctx.gmg_info()["n_free"][-1] == len(h.free[-1]) > 1000 - 8
+    r = np.random.default_rng(10).standard_normal(len(bc.free))
+    rf = np.zeros(bc.ndof)
+    rf[bc.free] = r
+    z = ctx.gmg_apply(_t(rf)).cpu().numpy()
+    assert _rel(z[bc.free], h.apply(r)) < 1e-10
+
+
 def _stencil_to_csr(S, dims):
     """(27,3,3,nnodes) stencil -> CSR over all DoFs of the level grid."""
     import scipy.sparse as sp

@@ -475,11 +475,11 @@ void dense_assemble(const Grid& g, const double* S, const int* dof_index, int n,
 // read as L afterwards.
 constexpr int CNB = 32;
 
-// One panel step. Every CTA factors the (k,k) block in shared memory (the
-// same arithmetic in each, so all agree): per pivot j one barrier; the
-// trailing entries of the working block take W[i][c] -= W[i][j] W[c][j] / d
-// while column j itself is only read, and its scaled values (sqrt(d) on the
-// diagonal, W[i][j] * rsqrt(d) below) go to a separate output block L. CTA 0
+// One panel step. Every CTA factors the (k,k) block in one warp's registers
+// (the same arithmetic in each, so all agree): per pivot j the trailing
+// entries take W[i][c] -= W[c][j] (W[i][j] / d) while column j itself is only
+// read, and its scaled values (sqrt(d) on the diagonal, W[i][j] * rsqrt(d)
+// below) go to a separate output block L in shared memory. CTA 0
 // stores L in Dt and raises `flag` on a non-positive or non-finite pivot (the
 // pivot is then taken as 1). The block is identity-padded past n, so every
 // loop below runs over the full 32 without predicates. Each thread then
@@ -490,7 +490,6 @@ __global__ void __launch_bounds__(128) k_chol_step(int n, int k, int band, doubl
   __shared__ double W[CNB][CNB + 1];
   __shared__ double L[CNB][CNB + 1];
   __shared__ double invd[CNB];
-  __shared__ double colj[CNB + 1];  // column j of the pivot step, then rsqrt(d)
   const int nb = min(CNB, n - k);
   const int tid = threadIdx.x;
   for (int q = tid; q < CNB * CNB; q += blockDim.x) {
@@ -498,45 +497,39 @@ __global__ void __launch_bounds__(128) k_chol_step(int n, int k, int band, doubl
     W[i][j] = (i < nb && j < nb && j <= i) ? A[(long long)(k + i) * n + k + j] : (i == j ? 1.0 : 0.0);
   }
   __syncthreads();
-  // warp 0 factors with lane cc holding column cc of the block in
-  // registers. Per pivot j (fully unrolled, so register indices are
-  // compile-time): lane j evaluates rsqrt(d) once and publishes its column in
-  // shared memory; every lane then reads that column with broadcast loads
-  // (no read-after-write through shared memory inside the update) and
-  // updates its own column in registers.
+  // warp 0 factors with lane r holding row r of the block in registers
+  // (wr[t] = W[r][t], t <= r). Per pivot j (fully unrolled, so register
+  // indices are compile-time): every lane takes d = W[j][j] from lane j by a
+  // shuffle and evaluates rsqrt(d) itself, its own multiplier W[r][j] / d is
+  // local, and the column entries W[t][j] arrive by shuffles from lanes t and
+  // are consumed at once: W[r][t] -= W[t][j] W[r][j] / d for j < t <= r. No
+  // shared memory and no warp barrier on the pivot chain.
   bool bad = false;
   if (tid < 32) {
     const int lane = tid;
-    double wc[CNB];
+    double wr[CNB];
 #pragma unroll
-    for (int i = 0; i < CNB; ++i) wc[i] = W[i][lane];
+    for (int t = 0; t < CNB; ++t) wr[t] = W[lane][t];
 #pragma unroll
     for (int j = 0; j < CNB; ++j) {
+      const double d = __shfl_sync(0xffffffffu, wr[j], j);
+      const bool ok = d > 0.0 && isfinite(d);
+      const double dd = ok ? d : 1.0;
+      const double rs = rsqrt(dd);
+      const double lj = wr[j];
       if (lane == j) {
-        const double d = wc[j];
-        const bool ok = d > 0.0 && isfinite(d);
-        const double dd = ok ? d : 1.0;
-        const double rs = rsqrt(dd);
-        colj[CNB] = rs;
         bad |= !ok;
-#pragma unroll
-        for (int i = j + 1; i < CNB; ++i) colj[i] = wc[i];
         L[j][j] = dd * rs;
         invd[j] = rs;
+      } else {
+        L[lane][j] = lane > j ? lj * rs : 0.0;
       }
-      __syncwarp();
-      const double rs = colj[CNB];
-      if (lane > j) {
-        const double lj = colj[lane];
-        L[lane][j] = lj * rs;
-        const double w = lj * (rs * rs);
+      const double w = lj * (rs * rs);
 #pragma unroll
-        for (int i = j + 1; i < CNB; ++i)
-          if (i >= lane) wc[i] -= colj[i] * w;
-      } else if (lane < j) {
-        L[lane][j] = 0.0;
+      for (int t = j + 1; t < CNB; ++t) {
+        const double ct = __shfl_sync(0xffffffffu, wr[j], t);
+        if (t <= lane) wr[t] -= ct * w;
       }
-      __syncwarp();
     }
     bad = __any_sync(0xffffffffu, bad);
   }
@@ -781,82 +774,117 @@ void dense_inverse_factor(int n, int band, const double* A, const double* Dt, do
 // combined matrix C (W below and on the diagonal, W^T above): pass one
 // y = W r_c (row i reads C[i][0..i]), pass two z_c = W^T y (row j reads
 // C[j][j..n-1]). One warp per row, 16-byte loads (rows are padded to ldc, a
-// multiple of 32 elements, so every row starts 16-byte aligned), FP64
-// accumulation, the compact vector staged in shared memory.
-template <typename T, typename TX>
-__global__ void k_coarse_lower(int n, long long ldc, const TX* __restrict__ C, const int* __restrict__ free_list,
-                               const T* __restrict__ rhs, double* __restrict__ y, const KrylovState* st) {
+// multiple of 32 elements, so every row starts 16-byte aligned), two loads in
+// flight per lane, FP64 accumulation. The compact right-hand side is gathered
+// once (k_coarse_gather) and both passes read the compact vectors straight
+// from global memory: they are n doubles, which every SM keeps in L1, so no
+// block spends its first microseconds staging them.
+template <typename T>
+__global__ void k_coarse_gather(int n, const int* __restrict__ free_list, const T* __restrict__ rhs,
+                                double* __restrict__ rc, const KrylovState* st) {
   if (st != nullptr && st->done) return;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  double* rc = reinterpret_cast<double*>(smem_raw);
-  for (int j = threadIdx.x; j < n; j += blockDim.x) rc[j] = (double)rhs[free_list[j]];
-  __syncthreads();
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j < n) rc[j] = (double)rhs[free_list[j]];
+}
+
+template <typename TX>
+__global__ void __launch_bounds__(256) k_coarse_lower(int n, long long ldc, const TX* __restrict__ C,
+                                                      const double* __restrict__ rc, double* __restrict__ y,
+                                                      const KrylovState* st) {
+  if (st != nullptr && st->done) return;
   const int row = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
   if (row >= n) return;
   constexpr int V = 16 / sizeof(TX);
   const TX* Ci = C + (long long)row * ldc;
   double acc = 0.0;
-  for (int j = lane * V; j <= row; j += 32 * V) {
+  int j = lane * V;
+  for (; j + 32 * V <= row; j += 64 * V) {  // two 16-byte loads in flight
+    TX v[V], w[V];
+    *reinterpret_cast<uint4*>(v) = __ldg(reinterpret_cast<const uint4*>(Ci + j));
+    const bool two = j + 32 * V <= row;
+    if (two) *reinterpret_cast<uint4*>(w) = __ldg(reinterpret_cast<const uint4*>(Ci + j + 32 * V));
+#pragma unroll
+    for (int q = 0; q < V; ++q) acc += (double)v[q] * __ldg(rc + j + q);
+    if (two) {
+#pragma unroll
+      for (int q = 0; q < V; ++q)
+        if (j + 32 * V + q <= row) acc += (double)w[q] * __ldg(rc + j + 32 * V + q);
+    }
+  }
+  for (; j <= row; j += 32 * V) {
     TX v[V];
-    *reinterpret_cast<uint4*>(v) = *reinterpret_cast<const uint4*>(Ci + j);
+    *reinterpret_cast<uint4*>(v) = __ldg(reinterpret_cast<const uint4*>(Ci + j));
 #pragma unroll
     for (int q = 0; q < V; ++q)
-      if (j + q <= row) acc += (double)v[q] * rc[j + q];
+      if (j + q <= row) acc += (double)v[q] * __ldg(rc + j + q);
   }
   acc = warp_sum(acc);
   if (lane == 0) y[row] = acc;
 }
 
 template <typename T, typename TX>
-__global__ void k_coarse_upper(int n, long long ldc, const TX* __restrict__ C, const int* __restrict__ free_list,
-                               const double* __restrict__ y, T* __restrict__ x, const KrylovState* st) {
+__global__ void __launch_bounds__(256) k_coarse_upper(int n, long long ldc, const TX* __restrict__ C,
+                                                      const int* __restrict__ free_list,
+                                                      const double* __restrict__ y, T* __restrict__ x,
+                                                      const KrylovState* st) {
   if (st != nullptr && st->done) return;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  double* ys = reinterpret_cast<double*>(smem_raw);
-  for (int j = threadIdx.x; j < n; j += blockDim.x) ys[j] = y[j];
-  __syncthreads();
   const int row = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
   if (row >= n) return;
   constexpr int V = 16 / sizeof(TX);
   const TX* Cj = C + (long long)row * ldc;
   double acc = 0.0;
-  for (int i = (row / V) * V + lane * V; i < n; i += 32 * V) {
-    TX v[V];
-    *reinterpret_cast<uint4*>(v) = *reinterpret_cast<const uint4*>(Cj + i);
+  int i = (row / V) * V + lane * V;
+  for (; i + 32 * V < n; i += 64 * V) {  // two 16-byte loads in flight
+    TX v[V], w[V];
+    *reinterpret_cast<uint4*>(v) = __ldg(reinterpret_cast<const uint4*>(Cj + i));
+    const bool two = i + 32 * V < n;
+    if (two) *reinterpret_cast<uint4*>(w) = __ldg(reinterpret_cast<const uint4*>(Cj + i + 32 * V));
 #pragma unroll
     for (int q = 0; q < V; ++q)
-      if (i + q >= row && i + q < n) acc += (double)v[q] * ys[i + q];
+      if (i + q >= row) acc += (double)v[q] * __ldg(y + i + q);
+    if (two) {
+#pragma unroll
+      for (int q = 0; q < V; ++q)
+        if (i + 32 * V + q < n) acc += (double)w[q] * __ldg(y + i + 32 * V + q);
+    }
+  }
+  for (; i < n; i += 32 * V) {
+    TX v[V];
+    *reinterpret_cast<uint4*>(v) = __ldg(reinterpret_cast<const uint4*>(Cj + i));
+#pragma unroll
+    for (int q = 0; q < V; ++q)
+      if (i + q >= row && i + q < n) acc += (double)v[q] * __ldg(y + i + q);
   }
   acc = warp_sum(acc);
   if (lane == 0) x[free_list[row]] = (T)acc;
 }
 
-// The compact vectors are staged in shared memory: opt in to more than 48 KB
-// when the coarsest system is large (B200 allows up to 227 KB per block).
+// The tri-inverse kernel stages column panels in shared memory beyond 48 KB.
 void dense_apply_prepare(int n) {
-  const int b = (int)(sizeof(double) * n);
-  if (b > 227 * 1024) throw std::runtime_error("coarsest system too large for the shared-memory solve");
-  const int a = std::max(b, 48 * 1024);
-  TOPO_CUDA_CHECK(cudaFuncSetAttribute(k_coarse_lower<double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, a));
-  TOPO_CUDA_CHECK(cudaFuncSetAttribute(k_coarse_lower<float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, a));
-  TOPO_CUDA_CHECK(cudaFuncSetAttribute(k_coarse_upper<double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, a));
-  TOPO_CUDA_CHECK(cudaFuncSetAttribute(k_coarse_upper<float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, a));
+  (void)n;
   TOPO_CUDA_CHECK(cudaFuncSetAttribute(k_tri_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TRI_SMEM));
 }
 
+// work: 2n doubles (y, then the compact right-hand side).
 void dense_apply(bool vec64, int n, long long ldc, const double* C64, const float* C32, const int* free_list,
-                 const void* rhs, double* y, void* x, const KrylovState* st, cudaStream_t s) {
+                 const void* rhs, double* work, void* x, const KrylovState* st, cudaStream_t s) {
   const int wpb = 8;
   const unsigned nb = (unsigned)((n + wpb - 1) / wpb);
-  const size_t sh = sizeof(double) * n;
+  double* y = work;
+  double* rc = work + n;
+  const unsigned ng = (unsigned)((n + 255) / 256);
   if (vec64) {
-    k_coarse_lower<double, double><<<nb, 32 * wpb, sh, s>>>(n, ldc, C64, free_list, (const double*)rhs, y, st);
+    k_coarse_gather<double><<<ng, 256, 0, s>>>(n, free_list, (const double*)rhs, rc, st);
     TOPO_LAUNCH_CHECK();
-    k_coarse_upper<double, double><<<nb, 32 * wpb, sh, s>>>(n, ldc, C64, free_list, y, (double*)x, st);
+    k_coarse_lower<double><<<nb, 32 * wpb, 0, s>>>(n, ldc, C64, rc, y, st);
+    TOPO_LAUNCH_CHECK();
+    k_coarse_upper<double, double><<<nb, 32 * wpb, 0, s>>>(n, ldc, C64, free_list, y, (double*)x, st);
   } else {
-    k_coarse_lower<float, float><<<nb, 32 * wpb, sh, s>>>(n, ldc, C32, free_list, (const float*)rhs, y, st);
+    k_coarse_gather<float><<<ng, 256, 0, s>>>(n, free_list, (const float*)rhs, rc, st);
     TOPO_LAUNCH_CHECK();
-    k_coarse_upper<float, float><<<nb, 32 * wpb, sh, s>>>(n, ldc, C32, free_list, y, (float*)x, st);
+    k_coarse_lower<float><<<nb, 32 * wpb, 0, s>>>(n, ldc, C32, rc, y, st);
+    TOPO_LAUNCH_CHECK();
+    k_coarse_upper<float, float><<<nb, 32 * wpb, 0, s>>>(n, ldc, C32, free_list, y, (float*)x, st);
   }
   TOPO_LAUNCH_CHECK();
 }

@@ -1231,7 +1231,7 @@ int topo_set_problem(topo_ctx* c, const uint8_t* free_mask, const double* F, voi
         c->C.dof_index = c->alloc<int>(Lc.g.ndof);
         c->C.free_list = c->alloc<int>(std::max(n, 1));
         c->C.ldc = ((n + 31) / 32) * 32;
-        c->C.y = c->alloc<double>(std::max(n, 1));
+        c->C.y = c->alloc<double>(2 * (size_t)std::max(n, 1));  // y, then the compact rhs
         alloc_slot(c, c->C.cur);
         if (c->C.nxt.A) alloc_slot(c, c->C.nxt);
         dense_apply_prepare(n);
