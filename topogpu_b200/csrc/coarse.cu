@@ -614,76 +614,90 @@ __global__ void k_block_tri_inv(const double* __restrict__ Dt, double* __restric
   for (int q = threadIdx.x; q < CNB * CNB; q += blockDim.x) Di[base + q] = X[q / CNB][q % CNB];
 }
 
-// W = L^-1 by block forward substitution in CNB-row steps. CTA J owns the
-// column block J; for I = J .. nT-1
-//   R    = delta_IJ Id - sum_{k in [max(32J, 32I-band), 32I)} L[32I.., k] W[k, 32J..]
-//   W_IJ = Di_I R
+// W = L^-1 by forward substitution, one strip of TWC columns per CTA. Every
+// column of W is an independent forward substitution, so the strips need no
+// communication: CTA J owns columns [TWC J, TWC J + TWC) and walks the
+// CNB-row blocks I from the one holding its first column to the last:
+//   R    = E - sum_{k in [max(j0, 32I-band), 32I)} L[32I.., k] W[k, strip]
+//   W_I  = Di_I R                    (E: the identity on these rows/columns)
 // Every W read is of rows this CTA wrote in an earlier step (visible after
-// __syncthreads), so the column blocks run independently with no grid sync;
-// the chain of column block 0 (nT steps) is the critical path, so each CTA
-// has an SM to itself (about 118 KB of shared memory).
-// The K range of a step is staged in 64-wide chunks (next chunk prefetched
-// into registers). Warp w takes the chunk rows k = w, w+8, ...; lane r keeps
-// row r of the 32x32 partial product (32 accumulators) and reads the W row
-// as broadcast 16-byte loads, so each shared-memory wavefront feeds 32 or
-// more FMAs. The 8 warp partials are summed through shared memory.
+// __syncthreads). The strip of column 0 is the critical path (nT steps), so
+// strips are narrower than a row block (16 columns; 32 and 8 measured
+// slower): a step is mostly the latency of its L reads, which come from L2
+// (all strips at block row I read the same L rows), in 64-wide chunks with
+// the next chunk prefetched into registers.
+// Warp w takes the chunk rows k = w, w+8, ...; lane r keeps row r of the
+// 32 x TWC partial product and reads the W row as broadcast loads; the 8 warp
+// partials are summed through shared memory.
 // W goes to W64 (lower part, FP64) and to the apply matrices C64 / C32 as W
 // in the lower triangle and W^T in the strict upper triangle, all with row
 // stride ldc.
-constexpr int TIT = 256, TKC = 64;
+constexpr int TIT = 256, TKC = 64, TWC = 16;
 struct TriSmem {
   double Ls[CNB][TKC + 1];
-  double Wc[TKC][CNB];
-  double red[TIT / 32][CNB][CNB + 1];
-  double Rs[CNB][CNB + 1];
+  double Wc[TKC][TWC];
+  double red[TIT / 32][CNB][TWC + 1];
+  double Rs[CNB][TWC + 1];
   double Ds[CNB][CNB + 1];
 };
 constexpr size_t TRI_SMEM = sizeof(TriSmem);
 
-__global__ void __launch_bounds__(TIT, 1) k_tri_inverse(int n, int band, const double* __restrict__ L,
-                                                        const double* __restrict__ Di, double* W64, long long ldc,
-                                                        double* C64, float* C32) {
+__global__ void __launch_bounds__(TIT) k_tri_inverse(int n, int band, const double* __restrict__ L,
+                                                     const double* __restrict__ Di, double* W64, long long ldc,
+                                                     double* C64, float* C32) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   TriSmem& S = *reinterpret_cast<TriSmem*>(smem_raw);
-  const int J = blockIdx.x, nT = gridDim.x;
+  const int nT = (n + CNB - 1) / CNB;
   const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
-  const int r = t >> 3, cq = (t & 7) * 4;
-  const int j0 = J * CNB;
-  double pl[8], pw[8];
-  for (int I = J; I < nT; ++I) {
+  const int j0 = blockIdx.x * TWC;
+  if (j0 >= n) return;  // uniform over the CTA
+  constexpr int PL = CNB * TKC / TIT;  // L values fetched per thread per chunk
+  constexpr int PW = TKC * TWC / TIT;  // W values fetched per thread per chunk
+  constexpr int PO = CNB * TWC / TIT;  // outputs per thread per step
+  static_assert(PL * TIT == CNB * TKC && PW * TIT == TKC * TWC && PO * TIT == CNB * TWC, "tile split");
+  double pl[PL], pw[PW];
+  for (int I = j0 / CNB; I < nT; ++I) {
     const int i0 = I * CNB;
     const int klo = max(j0, i0 - band);
     auto fetch = [&](int k0) {
 #pragma unroll
-      for (int m = 0; m < 8; ++m) {
+      for (int m = 0; m < PL; ++m) {
         const int q = t + TIT * m;
-        const int i = i0 + (q >> 6), k = k0 + (q & 63);
+        const int i = i0 + q / TKC, k = k0 + q % TKC;
         pl[m] = (i < n && k < i0) ? L[(long long)i * n + k] : 0.0;
-        const int kw = k0 + (q >> 5), cw = j0 + (q & 31);
+      }
+#pragma unroll
+      for (int m = 0; m < PW; ++m) {
+        const int q = t + TIT * m;
+        const int kw = k0 + q / TWC, cw = j0 + q % TWC;
         pw[m] = (kw < i0 && cw < n && cw <= kw) ? W64[(long long)kw * ldc + cw] : 0.0;
       }
     };
-    double acc[CNB];
+    double acc[TWC];
 #pragma unroll
-    for (int c = 0; c < CNB; ++c) acc[c] = 0.0;
+    for (int c = 0; c < TWC; ++c) acc[c] = 0.0;
     if (klo < i0) fetch(klo);
     for (int k0 = klo; k0 < i0; k0 += TKC) {
       __syncthreads();
 #pragma unroll
-      for (int m = 0; m < 8; ++m) {
+      for (int m = 0; m < PL; ++m) {
         const int q = t + TIT * m;
-        S.Ls[q >> 6][q & 63] = pl[m];
-        S.Wc[q >> 5][q & 31] = pw[m];
+        S.Ls[q / TKC][q % TKC] = pl[m];
+      }
+#pragma unroll
+      for (int m = 0; m < PW; ++m) {
+        const int q = t + TIT * m;
+        S.Wc[q / TWC][q % TWC] = pw[m];
       }
       __syncthreads();
       if (k0 + TKC < i0) fetch(k0 + TKC);
-#pragma unroll 2
+#pragma unroll 4
       for (int m = 0; m < TKC / 8; ++m) {
         const int kk = warp + 8 * m;
         const double a = S.Ls[lane][kk];
         const double2* wr = reinterpret_cast<const double2*>(&S.Wc[kk][0]);
 #pragma unroll
-        for (int c2 = 0; c2 < CNB / 2; ++c2) {
+        for (int c2 = 0; c2 < TWC / 2; ++c2) {
           const double2 w = wr[c2];
           acc[2 * c2] = fma(a, w.x, acc[2 * c2]);
           acc[2 * c2 + 1] = fma(a, w.y, acc[2 * c2 + 1]);
@@ -691,44 +705,48 @@ __global__ void __launch_bounds__(TIT, 1) k_tri_inverse(int n, int band, const d
       }
     }
 #pragma unroll
-    for (int c = 0; c < CNB; ++c) S.red[warp][lane][c] = acc[c];
+    for (int c = 0; c < TWC; ++c) S.red[warp][lane][c] = acc[c];
     for (int q = t; q < CNB * CNB; q += TIT) S.Ds[q >> 5][q & 31] = Di[(long long)I * CNB * CNB + q];
     __syncthreads();
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      double v = (i0 + r == j0 + cq + q) ? 1.0 : 0.0;
+    for (int p = 0; p < PO; ++p) {
+      const int q = t + TIT * p;
+      const int r = q / TWC, c = q % TWC;
+      double v = (i0 + r == j0 + c) ? 1.0 : 0.0;
 #pragma unroll
-      for (int w = 0; w < TIT / 32; ++w) v -= S.red[w][r][cq + q];
-      S.Rs[r][cq + q] = v;
+      for (int w = 0; w < TIT / 32; ++w) v -= S.red[w][r][c];
+      S.Rs[r][c] = v;
     }
     __syncthreads();
-    double w[4] = {0.0, 0.0, 0.0, 0.0};
-    for (int m = 0; m <= r; ++m) {
-      const double d = S.Ds[r][m];
+    double wv[PO];
 #pragma unroll
-      for (int q = 0; q < 4; ++q) w[q] = fma(d, S.Rs[m][cq + q], w[q]);
+    for (int p = 0; p < PO; ++p) {
+      const int q = t + TIT * p;
+      const int r = q / TWC, c = q % TWC;
+      double v = 0.0;
+      for (int m = 0; m <= r; ++m) v = fma(S.Ds[r][m], S.Rs[m][c], v);
+      wv[p] = v;
     }
     __syncthreads();
-    const int i = i0 + r;
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const int c = j0 + cq + q;
-      S.Rs[r][cq + q] = w[q];
-      if (i < n && c < n && c <= i) {
-        W64[(long long)i * ldc + c] = w[q];
-        if (C64 != nullptr && C64 != W64) C64[(long long)i * ldc + c] = w[q];
-        if (C32 != nullptr) C32[(long long)i * ldc + c] = (float)w[q];
+    for (int p = 0; p < PO; ++p) {
+      const int q = t + TIT * p;
+      const int r = q / TWC, c = q % TWC;
+      const int i = i0 + r, col = j0 + c;
+      S.Rs[r][c] = wv[p];
+      if (i < n && col < n && col <= i) {
+        W64[(long long)i * ldc + col] = wv[p];
+        if (C64 != nullptr && C64 != W64) C64[(long long)i * ldc + col] = wv[p];
+        if (C32 != nullptr) C32[(long long)i * ldc + col] = (float)wv[p];
       }
     }
     __syncthreads();
-    // transposed copy: thread -> row j0 + (t >> 3), columns i0 + (t & 7) * 4 + q
+    // transposed copy: rows j0 .. j0+TWC-1 of the upper triangle, columns i0 .. i0+31
     if (C64 != nullptr || C32 != nullptr) {
-      const int cr = j0 + r;
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int ic = i0 + cq + q;
+      for (int q = t; q < TWC * CNB; q += TIT) {
+        const int cr = j0 + q / CNB, ic = i0 + q % CNB;
         if (cr < n && ic < n && ic > cr) {
-          const double v = S.Rs[cq + q][r];
+          const double v = S.Rs[q % CNB][q / CNB];
           if (C64 != nullptr) C64[(long long)cr * ldc + ic] = v;
           if (C32 != nullptr) C32[(long long)cr * ldc + ic] = (float)v;
         }
@@ -766,7 +784,7 @@ void dense_inverse_factor(int n, int band, const double* A, const double* Dt, do
   const int nT = (n + CNB - 1) / CNB;
   k_block_tri_inv<<<nT, CNB, 0, s>>>(Dt, Di);
   TOPO_LAUNCH_CHECK();
-  k_tri_inverse<<<nT, TIT, TRI_SMEM, s>>>(n, band, A, Di, W64, ldc, C64, C32);
+  k_tri_inverse<<<(n + TWC - 1) / TWC, TIT, TRI_SMEM, s>>>(n, band, A, Di, W64, ldc, C64, C32);
   TOPO_LAUNCH_CHECK();
 }
 
