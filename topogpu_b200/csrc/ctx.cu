@@ -210,6 +210,7 @@ struct topo_ctx {
   double* dtmp = nullptr;       // 64 device doubles
   double* oc_state = nullptr;
   double* Hs = nullptr;
+  FilterStencil fstencil;
   cudaStream_t cs = nullptr;
   cudaEvent_t ev_in = nullptr, ev_out = nullptr;
   cudaEvent_t ev_ph[6] = {};     // setup phase marks (timed)
@@ -1121,6 +1122,8 @@ int topo_ctx_create(int nelx, int nely, int nelz, int n_levels, int mode, int fi
     c->dtmp = c->alloc<double>(64);
     c->oc_state = c->alloc<double>(16);
     c->Hs = c->alloc<double>(g0.nelem);
+    c->fstencil.off = c->alloc<int>(3 * kMaxFilterOff);
+    c->fstencil.w = c->alloc<double>(kMaxFilterOff);
     // largest coarse-level vector for FP64 scratch (used when vectors are FP32)
     long long maxc = 1;
     for (int l = 1; l < n_levels; ++l) maxc = std::max(maxc, c->L[l].g.ndof);
@@ -1433,7 +1436,7 @@ int topo_filter(topo_ctx* c, double rmin, const double* in, double* out, int tra
     if (!(rmin > 0.0)) throw std::invalid_argument("topo_filter: rmin must be > 0");
     if (in == out) throw std::invalid_argument("topo_filter: in and out must differ");
     StreamGuard sg(c, stream);
-    filter_apply(c->L[0].g, rmin, in, out, transpose != 0, c->Hs, c->cs);
+    filter_apply(c->fstencil, c->L[0].g, rmin, in, out, transpose != 0, c->Hs, c->cs);
     return 0;
   } catch (const std::exception& e) {
     return fail(c, e);
@@ -1489,7 +1492,7 @@ int topo_oc_projected(topo_ctx* c, double rmin, const double* rho, const double*
     if (out == rho || out == dc || out == dv)
       throw std::invalid_argument("topo_oc_projected: out must not alias rho, dc or dv");
     StreamGuard sg(c, stream);
-    const int ev = oc_update_projected(c->L[0].g, rmin, rho, dc, dv, beta, eta, volfrac, move, rho_min, out, c->Hs,
+    const int ev = oc_update_projected(c->fstencil, c->L[0].g, rmin, rho, dc, dv, beta, eta, volfrac, move, rho_min, out, c->Hs,
                                        c->red, c->oc_state, c->cs);
     if (out_evals) *out_evals = ev;
     return 0;

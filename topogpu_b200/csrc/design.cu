@@ -16,21 +16,11 @@
 
 namespace topo {
 
-constexpr int kMaxFilterOff = 1331;  // (2*5+1)^3: rmin < 6
-__constant__ int cFoff[kMaxFilterOff][3];
-__constant__ double cFw[kMaxFilterOff];
-
-struct FilterStencil {
-  double rmin = -1.0;
-  int n = 0;
-};
-static FilterStencil g_filter;
-
 // Offsets and weights of the linear-hat filter: every element at centre
 // distance d <= rmin - 1e-10 with weight rmin - d, plus the element itself with
 // weight rmin (pub_simp_solver.py:215-243; kd-tree query_pairs radius).
-static void set_filter(double rmin, cudaStream_t s) {
-  if (g_filter.rmin == rmin) return;
+static void set_filter(FilterStencil& fs, double rmin, cudaStream_t s) {
+  if (fs.rmin == rmin) return;
   const int R = (int)std::floor(rmin);
   std::vector<int> off;
   std::vector<double> w;
@@ -47,33 +37,36 @@ static void set_filter(double rmin, cudaStream_t s) {
         }
       }
   if ((int)w.size() > kMaxFilterOff) throw std::runtime_error("filter radius too large (rmin must be < 6)");
-  TOPO_CUDA_CHECK(cudaMemcpyToSymbolAsync(cFoff, off.data(), sizeof(int) * off.size(), 0, cudaMemcpyHostToDevice, s));
-  TOPO_CUDA_CHECK(cudaMemcpyToSymbolAsync(cFw, w.data(), sizeof(double) * w.size(), 0, cudaMemcpyHostToDevice, s));
+  TOPO_CUDA_CHECK(cudaMemcpyAsync(fs.off, off.data(), sizeof(int) * off.size(), cudaMemcpyHostToDevice, s));
+  TOPO_CUDA_CHECK(cudaMemcpyAsync(fs.w, w.data(), sizeof(double) * w.size(), cudaMemcpyHostToDevice, s));
   TOPO_CUDA_CHECK(cudaStreamSynchronize(s));
-  g_filter.rmin = rmin;
-  g_filter.n = (int)w.size();
+  fs.rmin = rmin;
+  fs.n = (int)w.size();
 }
 
-__device__ __forceinline__ double row_weight_sum(const Grid& g, int ex, int ey, int ez, int noff) {
+__device__ __forceinline__ double row_weight_sum(const Grid& g, int ex, int ey, int ez, int noff,
+                                                 const int* __restrict__ fo, const double* __restrict__ fw) {
   double hs = 0.0;
   for (int k = 0; k < noff; ++k) {
-    const int x = ex + cFoff[k][0], y = ey + cFoff[k][1], z = ez + cFoff[k][2];
-    if (x >= 0 && x < g.nx && y >= 0 && y < g.ny && z >= 0 && z < g.nz) hs += cFw[k];
+    const int x = ex + fo[3 * k], y = ey + fo[3 * k + 1], z = ez + fo[3 * k + 2];
+    if (x >= 0 && x < g.nx && y >= 0 && y < g.ny && z >= 0 && z < g.nz) hs += fw[k];
   }
   return hs;
 }
 
-__global__ void k_filter_rowsum(Grid g, int noff, double* __restrict__ Hs) {
+__global__ void k_filter_rowsum(Grid g, int noff, const int* __restrict__ fo, const double* __restrict__ fw,
+                                double* __restrict__ Hs) {
   const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (e >= g.nelem) return;
   const int ez = e % g.nz, ey = (e / g.nz) % g.ny, ex = e / ((long long)g.nz * g.ny);
-  Hs[e] = row_weight_sum(g, ex, ey, ez, noff);
+  Hs[e] = row_weight_sum(g, ex, ey, ez, noff, fo, fw);
 }
 
 // out_i = sum_j (w_ij / Hs_i) in_j          (transpose = 0)
 // out_j = sum_i (w_ij / Hs_i) in_i          (transpose = 1)
-__global__ void k_filter(Grid g, int noff, const double* __restrict__ in, double* __restrict__ out,
-                         const double* __restrict__ Hs, int transpose) {
+__global__ void k_filter(Grid g, int noff, const int* __restrict__ fo, const double* __restrict__ fw,
+                         const double* __restrict__ in, double* __restrict__ out, const double* __restrict__ Hs,
+                         int transpose) {
   const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (e >= g.nelem) return;
   const int ez = e % g.nz, ey = (e / g.nz) % g.ny, ex = e / ((long long)g.nz * g.ny);
@@ -81,29 +74,29 @@ __global__ void k_filter(Grid g, int noff, const double* __restrict__ in, double
   if (!transpose) {
     const double hs = Hs[e];
     for (int k = 0; k < noff; ++k) {
-      const int x = ex + cFoff[k][0], y = ey + cFoff[k][1], z = ez + cFoff[k][2];
+      const int x = ex + fo[3 * k], y = ey + fo[3 * k + 1], z = ez + fo[3 * k + 2];
       if (x < 0 || x >= g.nx || y < 0 || y >= g.ny || z < 0 || z >= g.nz) continue;
-      acc += (cFw[k] / hs) * in[((long long)x * g.ny + y) * g.nz + z];
+      acc += (fw[k] / hs) * in[((long long)x * g.ny + y) * g.nz + z];
     }
   } else {
     for (int k = 0; k < noff; ++k) {
-      const int x = ex + cFoff[k][0], y = ey + cFoff[k][1], z = ez + cFoff[k][2];
+      const int x = ex + fo[3 * k], y = ey + fo[3 * k + 1], z = ez + fo[3 * k + 2];
       if (x < 0 || x >= g.nx || y < 0 || y >= g.ny || z < 0 || z >= g.nz) continue;
       const long long i = ((long long)x * g.ny + y) * g.nz + z;
-      acc += (cFw[k] / Hs[i]) * in[i];
+      acc += (fw[k] / Hs[i]) * in[i];
     }
   }
   out[e] = acc;
 }
 
-void filter_apply(const Grid& g, double rmin, const double* in, double* out, bool transpose, double* Hs_work,
-                  cudaStream_t s) {
-  set_filter(rmin, s);
+void filter_apply(FilterStencil& fs, const Grid& g, double rmin, const double* in, double* out, bool transpose,
+                  double* Hs_work, cudaStream_t s) {
+  set_filter(fs, rmin, s);
   const int bs = 256;
   const unsigned nb = (unsigned)((g.nelem + bs - 1) / bs);
-  k_filter_rowsum<<<nb, bs, 0, s>>>(g, g_filter.n, Hs_work);
+  k_filter_rowsum<<<nb, bs, 0, s>>>(g, fs.n, fs.off, fs.w, Hs_work);
   TOPO_LAUNCH_CHECK();
-  k_filter<<<nb, bs, 0, s>>>(g, g_filter.n, in, out, Hs_work, transpose ? 1 : 0);
+  k_filter<<<nb, bs, 0, s>>>(g, fs.n, fs.off, fs.w, in, out, Hs_work, transpose ? 1 : 0);
   TOPO_LAUNCH_CHECK();
 }
 
@@ -334,8 +327,9 @@ __global__ void k_ocp_cand(long long n, const double* __restrict__ rho, const do
     cand[i] = ocf_candidate(rho[i], dc[i], dv[i], lm, move, rho_min);
 }
 
-__global__ void k_ocp_vol(Grid g, int noff, const double* __restrict__ cand, const double* __restrict__ Hs,
-                          Projection p, double volfrac, double* st, RedWork red) {
+__global__ void k_ocp_vol(Grid g, int noff, const int* __restrict__ fo, const double* __restrict__ fw,
+                          const double* __restrict__ cand, const double* __restrict__ Hs, Projection p,
+                          double volfrac, double* st, RedWork red) {
   if (st[OF_DONE] != 0.0) return;
   const double lm = st[OF_LM];
   double v[1] = {0.0};
@@ -345,9 +339,9 @@ __global__ void k_ocp_vol(Grid g, int noff, const double* __restrict__ cand, con
     const double hs = Hs[e];
     double acc = 0.0;
     for (int k = 0; k < noff; ++k) {
-      const int x = ex + cFoff[k][0], y = ey + cFoff[k][1], z = ez + cFoff[k][2];
+      const int x = ex + fo[3 * k], y = ey + fo[3 * k + 1], z = ez + fo[3 * k + 2];
       if (x < 0 || x >= g.nx || y < 0 || y >= g.ny || z < 0 || z >= g.nz) continue;
-      acc += (cFw[k] / hs) * cand[((long long)x * g.ny + y) * g.nz + z];
+      acc += (fw[k] / hs) * cand[((long long)x * g.ny + y) * g.nz + z];
     }
     v[0] += p.on ? (p.tbe + tanh(p.beta * (acc - p.eta))) / p.den : acc;
   }
@@ -363,14 +357,14 @@ __global__ void k_ocp_vol(Grid g, int noff, const double* __restrict__ cand, con
   }
 }
 
-int oc_update_projected(const Grid& g, double rmin, const double* rho, const double* dc, const double* dv,
+int oc_update_projected(FilterStencil& fs, const Grid& g, double rmin, const double* rho, const double* dc, const double* dv,
                         double beta, double eta, double volfrac, double move, double rho_min, double* out,
                         double* Hs_work, RedWork red, double* st, cudaStream_t s) {
   const long long n = g.nelem;
-  set_filter(rmin, s);
+  set_filter(fs, rmin, s);
   const Projection p = make_projection(beta, eta);
   const unsigned nb = (unsigned)std::min<long long>(kRedBlocks, (n + kRedThreads - 1) / kRedThreads);
-  k_filter_rowsum<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(g, g_filter.n, Hs_work);
+  k_filter_rowsum<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(g, fs.n, fs.off, fs.w, Hs_work);
   TOPO_LAUNCH_CHECK();
   k_ocf_init<<<1, 1, 0, s>>>(st);
   TOPO_LAUNCH_CHECK();
@@ -380,7 +374,7 @@ int oc_update_projected(const Grid& g, double rmin, const double* rho, const dou
     for (int k = 0; k < 16 && launched < 100; ++k, ++launched) {
       k_ocp_cand<<<nb, kRedThreads, 0, s>>>(n, rho, dc, dv, move, rho_min, st, out);
       TOPO_LAUNCH_CHECK();
-      k_ocp_vol<<<nb, kRedThreads, 0, s>>>(g, g_filter.n, out, Hs_work, p, volfrac, st, red);
+      k_ocp_vol<<<nb, kRedThreads, 0, s>>>(g, fs.n, fs.off, fs.w, out, Hs_work, p, volfrac, st, red);
       TOPO_LAUNCH_CHECK();
     }
     TOPO_CUDA_CHECK(cudaMemcpyAsync(h, st, sizeof(double) * 16, cudaMemcpyDeviceToHost, s));

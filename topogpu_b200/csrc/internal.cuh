@@ -293,7 +293,17 @@ void scale_dev(bool f64, long long n, const void* x, const double* num, const do
                cudaStream_t s);
 
 // design (design.cu)
-void filter_apply(const Grid& g, double rmin, const double* in, double* out, bool transpose,
+// Offsets and weights of the linear-hat density filter for one radius, in
+// device memory owned by a context (so contexts with different radii, or on
+// different devices, never share it).
+constexpr int kMaxFilterOff = 1331;  // (2*5+1)^3: rmin < 6
+struct FilterStencil {
+  double rmin = -1.0;
+  int n = 0;
+  int* off = nullptr;    // 3 * kMaxFilterOff
+  double* w = nullptr;   // kMaxFilterOff
+};
+void filter_apply(FilterStencil& fs, const Grid& g, double rmin, const double* in, double* out, bool transpose,
                   double* Hs_work, cudaStream_t s);
 int oc_update(long long n, const double* rho, const double* dc, double volfrac, double move,
               double rho_min, double* out, RedWork red, double* state, cudaStream_t s);
@@ -302,7 +312,7 @@ int oc_update_filtered(long long n, const double* rho, const double* dc, const d
                        RedWork red, double* state, cudaStream_t s);
 void heaviside_apply(long long n, const double* rho_f, double beta, double eta, double* phys, double* dh,
                      cudaStream_t s);
-int oc_update_projected(const Grid& g, double rmin, const double* rho, const double* dc, const double* dv,
+int oc_update_projected(FilterStencil& fs, const Grid& g, double rmin, const double* rho, const double* dc, const double* dv,
                         double beta, double eta, double volfrac, double move, double rho_min, double* out,
                         double* Hs_work, RedWork red, double* st, cudaStream_t s);
 void field_stats(long long n, const double* x, double* out4_dev, RedWork red, cudaStream_t s);
