@@ -456,3 +456,17 @@ def test_probe_quality_and_kappa_eff_match_oracle(cuda_dev):
     ref = eig[-1] / eig[eig > 0][0]
     assert abs(kappa - ref) <= 1e-6 * ref, (kappa, ref)
     st.close()
+
+
+def test_different_element_stiffness_refused_while_shared_one_is_live(cuda_dev):
+    """KE sits in constant memory shared by every context of a device: a
+    context with another KE is refused while one with the default is alive,
+    and a second context with the same KE is accepted."""
+    from topogpu_b200.context import TopoContext
+    from topogpu_b200.fem import KE_UNIT
+
+    a = TopoContext((4, 2, 2), n_levels=1, mode="fp64")
+    with pytest.raises(RuntimeError, match="different element stiffness"):
+        TopoContext((4, 2, 2), n_levels=1, mode="fp64", KE=KE_UNIT * 2.0)
+    b = TopoContext((4, 2, 2), n_levels=1, mode="fp64", KE=KE_UNIT.copy())
+    assert a.ndof == b.ndof

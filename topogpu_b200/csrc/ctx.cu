@@ -211,6 +211,7 @@ struct topo_ctx {
   double* oc_state = nullptr;
   double* Hs = nullptr;
   FilterStencil fstencil;
+  bool ke_registered = false;  // holds a reference on its device's KE
   cudaStream_t cs = nullptr;
   cudaEvent_t ev_in = nullptr, ev_out = nullptr;
   cudaEvent_t ev_ph[6] = {};     // setup phase marks (timed)
@@ -1034,6 +1035,50 @@ int do_fgmres(topo_ctx* c, const double* b, double* x, double tol, int maxiter, 
 // ======================================================================
 extern "C" {
 
+// The element stiffness lives in constant memory (folded into the K.u
+// instructions as operands) and in the tensor-core B tile, one copy per
+// device shared by every context on it. The first live context of a device
+// uploads it; later contexts must use the same KE (a different one is
+// refused, since it would silently change the operator of the others) and
+// do not write it again while kernels of other contexts may be reading it.
+namespace {
+struct DeviceKE {
+  std::vector<double> ke;
+  int live = 0;
+};
+std::mutex g_ke_mu;
+std::vector<DeviceKE> g_ke;
+}  // namespace
+
+static void register_ke(topo_ctx* c, const double* KE) {
+  std::lock_guard<std::mutex> lk(g_ke_mu);
+  if ((int)g_ke.size() <= c->device) g_ke.resize(c->device + 1);
+  DeviceKE& d = g_ke[c->device];
+  if (d.live > 0) {
+    if (std::memcmp(d.ke.data(), KE, sizeof(double) * 576) != 0)
+      throw std::invalid_argument(
+          "topo_ctx_create: another live context on this device uses a different element stiffness KE "
+          "(KE is held in constant memory shared by all contexts of a device)");
+  } else {
+    set_ke(KE);
+    set_ke_block(KE);
+    std::vector<double> Q(8 * 576);
+    host_galerkin_q(KE, Q.data());
+    set_galerkin_q(Q.data());
+    tc_prepare(KE);
+    d.ke.assign(KE, KE + 576);
+  }
+  d.live += 1;
+  c->ke_registered = true;
+}
+
+static void release_ke(topo_ctx* c) {
+  if (!c->ke_registered) return;
+  std::lock_guard<std::mutex> lk(g_ke_mu);
+  if (c->device < (int)g_ke.size() && g_ke[c->device].live > 0) g_ke[c->device].live -= 1;
+  c->ke_registered = false;
+}
+
 int topo_version(void) { return 100; }
 
 int topo_ctx_create(int nelx, int nely, int nelz, int n_levels, int mode, int fine_degree, int coarse_degree,
@@ -1055,12 +1100,7 @@ int topo_ctx_create(int nelx, int nely, int nelz, int n_levels, int mode, int fi
     c->coarse_degree = coarse_degree;
     c->cheb_lower = cheb_lower;
     c->dense_max = dense_max;
-    set_ke(KE_host);
-    set_ke_block(KE_host);
-    std::vector<double> Q(8 * 576);
-    host_galerkin_q(KE_host, Q.data());
-    set_galerkin_q(Q.data());
-    tc_prepare(KE_host);
+    register_ke(c, KE_host);
     const char* no_tc = std::getenv("TOPO_B200_NO_TC");
     c->use_tc = !(no_tc && no_tc[0] == '1');
     TOPO_CUDA_CHECK(cudaStreamCreateWithFlags(&c->cs, cudaStreamNonBlocking));
@@ -1145,6 +1185,7 @@ int topo_ctx_destroy(topo_ctx* c) {
   if (!c) return 0;
   cudaSetDevice(c->device);
   if (c->cs) cudaStreamSynchronize(c->cs);
+  release_ke(c);
   for (void* p : c->allocs) cudaFree(p);
   if (c->h_st) cudaFreeHost(c->h_st);
   if (c->blk_Gh) cudaFreeHost(c->blk_Gh);
