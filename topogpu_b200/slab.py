@@ -199,10 +199,16 @@ class SlabPCG:
 
     def solve(self, b: torch.Tensor, x: torch.Tensor | None = None, tol=1e-8, maxiter=500):
         """Returns (x, iterations, relative residual, converged); b and x are
-        consistent slab vectors (FP64)."""
+        consistent slab vectors (FP64). Every rank must pass an initial x, or
+        every rank none."""
         world = self.slab.world
-        x = torch.zeros_like(b) if x is None else x
-        r = b - self.apply_K(x) if torch.any(x != 0) else b.clone()
+        # the branch depends only on the call (every rank passes x or none),
+        # never on this rank's data, so all ranks take the same exchanges
+        if x is None:
+            x = torch.zeros_like(b)
+            r = b.clone()
+        else:
+            r = b - self.apply_K(x)
         (bb,) = all_dots([(b, b)], self.w, self.dist, world)
         bn = max(np.sqrt(bb), 1e-300)
         z = self.apply_M(r)
