@@ -25,10 +25,13 @@ reference. Every array is produced by reference code paths:
                    projection at beta 1 (the SIMPParams default) and beta 8
   wcycle.npz       GalerkinMatFreeGMG(cycle_type="w").apply and PCG on the
                    galerkin.npz hierarchies
+  run_simp_control.npz  run_simp on its 3-D tip-load cantilever preset with
+                   a scripted controller (initial action, beta/penal/move
+                   changes, a restart from the best design, a stop, a tail)
   ckpt_24x12x6_cantilever.{npz,json}  the checkpoint run_simp writes after
                    iteration 2 of config 0 (checkpoint_every 1)
 
-``python make_golden.py [REF_ROOT] [--only heaviside|checkpoint|wcycle]``
+``python make_golden.py [REF_ROOT] [--only heaviside|checkpoint|wcycle|control]``
 regenerates all fixtures, or only the named group.
 """
 
@@ -229,7 +232,49 @@ def main(ref_root: str) -> None:
     heaviside_fixtures(ref_root)
     checkpoint_fixtures(ref_root)
     wcycle_fixtures(ref_root)
+    control_fixtures(ref_root)
     print("golden fixtures written to", HERE)
+
+
+class ScriptedController:
+    """Deterministic run_simp callback: the same script is replayed by the
+    tests against the B200 driver."""
+
+    def initial_action(self, params):
+        return {"move": 0.15}
+
+    def __call__(self, state, rho_new):
+        if state.iteration == 2:
+            return {"beta": 4.0, "penal": 3.5}
+        if state.iteration == 4:
+            return {"restart": True, "move": 0.1}
+        if state.iteration == 6:
+            return {"stop": True}
+        return None
+
+    def finalize_tail(self, params):
+        return {"enabled": True, "tail_iters": 2, "penal": 4.0, "move": 0.05, "beta": 8.0, "rmin": 1.2}
+
+
+def control_fixtures(ref_root) -> None:
+    _setup(Path(ref_root))
+    from gpu_fem.pub_simp_solver import SIMPParams, run_simp
+
+    params = SIMPParams(nelx=16, nely=8, nelz=4, volfrac=0.3, rmin=1.5, move=0.2, max_iter=10, min_iter=3,
+                        use_heaviside=True, beta_init=1.0, max_gray_for_best=0.9)
+    with redirect_stdout(io.StringIO()):
+        res = run_simp(params, callback=ScriptedController(), verbose=False)
+    log = res["params_log"]
+    d = {"compliance": np.array(res["compliance_history"]), "rho_final": res["rho_final"],
+         "best_rho": res["best_rho"], "best_compliance": np.array(res["best_compliance"]),
+         "best_iteration": np.array(res["best_iteration"]), "final_compliance": np.array(res["final_compliance"]),
+         "best_is_valid": np.array(int(res["best_is_valid"])), "n_iter": np.array(res["n_iter"]),
+         "log_iter": np.array([r["iter"] for r in log]), "log_tail": np.array([r["phase"] == "tail" for r in log]),
+         "log_penal": np.array([r["penal"] for r in log]), "log_rmin": np.array([r["rmin"] for r in log]),
+         "log_move": np.array([r["move"] for r in log]), "log_beta": np.array([r["beta"] for r in log]),
+         "log_gray": np.array([r["grayness"] for r in log]), "log_vf": np.array([r["volume_fraction"] for r in log]),
+         "pre_valid_best_compliance": np.array(res["pre_valid_best_compliance"])}
+    np.savez_compressed(HERE / "run_simp_control.npz", **d)
 
 
 def wcycle_fixtures(ref_root) -> None:
@@ -306,7 +351,7 @@ if __name__ == "__main__":
 
     ap = argparse.ArgumentParser()
     ap.add_argument("ref_root", nargs="?", default="/root/reference")
-    ap.add_argument("--only", choices=["heaviside", "checkpoint", "wcycle"], default=None)
+    ap.add_argument("--only", choices=["heaviside", "checkpoint", "wcycle", "control"], default=None)
     a = ap.parse_args()
     if a.only == "heaviside":
         heaviside_fixtures(a.ref_root)
@@ -314,5 +359,7 @@ if __name__ == "__main__":
         checkpoint_fixtures(a.ref_root)
     elif a.only == "wcycle":
         wcycle_fixtures(a.ref_root)
+    elif a.only == "control":
+        control_fixtures(a.ref_root)
     else:
         main(a.ref_root)

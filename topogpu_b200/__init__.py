@@ -27,6 +27,9 @@ _EXPORTS = {
     "MatrixFreeOperator": ("topogpu_b200.operators", "MatrixFreeOperator"),
     "GMGPreconditioner": ("topogpu_b200.operators", "GMGPreconditioner"),
     "StateSolver": ("topogpu_b200.state", "StateSolver"),
+    "run_simp": ("topogpu_b200.run_simp", "run_simp"),
+    "SIMPParams": ("topogpu_b200.run_simp", "SIMPParams"),
+    "StepState": ("topogpu_b200.run_simp", "StepState"),
     "OCOptimizer": ("topogpu_b200.solver", "OCOptimizer"),
     "OptimizationResult": ("topogpu_b200.solver", "OptimizationResult"),
     "SIMPModel": ("topogpu_b200.solver", "SIMPModel"),
