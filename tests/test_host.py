@@ -125,11 +125,12 @@ def test_evidence_bundle_manifest(tmp_path):
     assert head == "compliance,iteration,wall_s"
 
 
-def test_cpu_backend_is_rejected_loudly():
+def test_backend_and_optimizer_checks():
     import topogpu_b200 as tg
 
-    with pytest.raises(ValueError, match="GPU-only"):
-        tg.SIMPSolver(backend="cpu")
+    assert tg.SIMPSolver(backend="cpu").backend == "cpu"  # run_simp, physics on the GPU
+    with pytest.raises(ValueError, match="Unknown backend"):
+        tg.SIMPSolver(backend="tpu")
     with pytest.raises(ValueError, match="optimizer"):
         tg.SIMPSolver(optimizer="mma")
 

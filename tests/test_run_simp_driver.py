@@ -167,3 +167,23 @@ def test_driver_device_physics_matches_oracle_physics(cuda_dev):
     assert res["n_iter"] == ref["n_iter"]
     assert [r["beta"] for r in res["params_log"]] == [r["beta"] for r in ref["params_log"]]
     np.testing.assert_allclose(res["rho_final"], ref["rho_final"], atol=1e-5)
+
+
+@pytest.mark.gpu
+def test_simpsolver_cpu_backend_runs_run_simp_on_device(cuda_dev):
+    """SIMPSolver(backend="cpu") is the reference's run_simp path
+    (src/topogpu/solver.py:156-184) with the problem's own BCs: against the
+    driver with the oracle physics on the same parameters."""
+    import topogpu_b200 as tg
+    from topogpu_b200.bc import generate_bc
+    from topogpu_b200.run_simp import SIMPParams, run_simp
+
+    p = tg.gallery.benchmark_cantilever((16, 8, 4), volfrac=0.3, filter_radius=1.5)
+    res = tg.SIMPSolver(backend="cpu", max_iter=3, move=0.2).solve(p)
+    bc = generate_bc(p.spec)
+    F = p.force_override if p.force_override is not None else bc.F  # the loads SIMPSolver uses
+    params = SIMPParams(nelx=16, nely=8, nelz=4, volfrac=0.3, rmin=1.5, max_iter=3, min_iter=2, move=0.2, tol=1e-3)
+    ref = run_simp(params, fea=OracleFEA((16, 8, 4), bc.free_dofs, F))
+    np.testing.assert_allclose([r["compliance"] for r in res.history], ref["compliance_history"], rtol=1e-6)
+    assert res.summary["backend"] == "cpu" and res.summary["n_iter"] == ref["n_iter"]
+    np.testing.assert_allclose(res.rho_final, ref["rho_final"], atol=1e-5)

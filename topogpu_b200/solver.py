@@ -8,7 +8,9 @@ GMG setup, Krylov solve, compliance, sensitivity and the bisection OC update
 that go into the history rows.
 
 Defaults reproduce the reference path: no density filter, penalty 3,
-OC on the plain mean volume. ``use_filter=True`` switches to the filtered
+OC on the plain mean volume. ``backend="cpu"`` (the reference's CPU
+backend, ``run_simp``) runs that driver with its physics on the GPU
+(``topogpu_b200.run_simp``). ``use_filter=True`` switches to the filtered
 formulation of the reference's CPU driver ``run_simp``
 (src/gpu_fem/pub_simp_solver.py:342-377): physical density H rho,
 sensitivities chained through H^T, volume measured after the filter.
@@ -91,9 +93,7 @@ class SIMPSolver:
                  checkpoint_problem="cantilever", cycle_type="v", device=None):
         if optimizer != "oc":
             raise ValueError("Only optimizer='oc' is implemented in v0.1.0.")
-        if backend in {"cpu", "scipy"}:
-            raise ValueError("backend='cpu' is not part of topogpu_b200 (GPU-only build); use backend='cuda'.")
-        if backend not in {"cuda", "cupy"}:
+        if backend not in {"cuda", "cupy", "cpu", "scipy"}:
             raise ValueError(f"Unknown backend {backend!r}.")
         if linear_solver not in {"auto", "pcg_gmg", "fgmres_gmg"}:
             raise ValueError(f"Unknown linear_solver {linear_solver!r}.")
@@ -141,6 +141,8 @@ class SIMPSolver:
 
     def solve(self, problem: TopologyProblem) -> OptimizationResult:
         problem.validate()
+        if self.backend in {"cpu", "scipy"}:
+            return self._solve_run_simp(problem)
         loop = SIMPLoop(self, problem, track_best=self.checkpoint_dir is not None)
         try:
             ckpt_path = None
@@ -166,6 +168,32 @@ class SIMPSolver:
             return OptimizationResult(problem, loop.rho.cpu().numpy(), history, summary)
         finally:
             loop.close()
+
+
+    def _solve_run_simp(self, problem: TopologyProblem) -> OptimizationResult:
+        """The reference's ``backend="cpu"`` path (src/topogpu/solver.py:156-184):
+        ``run_simp`` with the same parameters (radius, move, tol 1e-3,
+        min_iter min(2, max_iter), Heaviside at beta 1), here with its physics
+        on the GPU. The problem's own supports and loads are used; the
+        reference drops them there and solves run_simp's tip-load preset."""
+        from .run_simp import SIMPParams, run_simp
+
+        spec = problem.spec
+        if not problem.is_3d:
+            raise ValueError("the B200 run_simp path handles 3-D problems only")
+        bc = generate_bc(spec)
+        F = problem.force_override if problem.force_override is not None else bc.F
+        params = SIMPParams(nelx=spec.nelx, nely=spec.nely, nelz=spec.nelz, volfrac=spec.volfrac,
+                            rmin=problem.filter_radius or spec.rmin or 1.5, max_iter=self.max_iter,
+                            min_iter=min(2, self.max_iter), move=self.move, tol=1.0e-3,
+                            checkpoint_dir=self.checkpoint_dir, checkpoint_every=self.checkpoint_every)
+        result = run_simp(params, verbose=False, bc_override=lambda a, b, c: (bc.fixed_dofs, bc.free_dofs, F),
+                          problem=self.checkpoint_problem, levels=self.levels, device=self.device)
+        history = [{"iteration": i + 1, "compliance": float(c)} for i, c in enumerate(result["compliance_history"])]
+        summary = {"problem": problem.to_dict(), "backend": "cpu", "linear_solver": "gmg_pcg_fp64_on_b200",
+                   "n_iter": int(result["n_iter"]), "final_compliance": float(result["final_compliance"]),
+                   "final_grayness": float(result["final_grayness"])}
+        return OptimizationResult(problem, result["rho_final"], history, summary)
 
 
 class SIMPLoop:
