@@ -28,10 +28,12 @@ reference. Every array is produced by reference code paths:
   run_simp_control.npz  run_simp on its 3-D tip-load cantilever preset with
                    a scripted controller (initial action, beta/penal/move
                    changes, a restart from the best design, a stop, a tail)
+  run_simp_resume.npz  run_simp on the 3-D preset interrupted after 4 of 7
+                   iterations (checkpoint_every 2) and resumed: both legs
   ckpt_24x12x6_cantilever.{npz,json}  the checkpoint run_simp writes after
                    iteration 2 of config 0 (checkpoint_every 1)
 
-``python make_golden.py [REF_ROOT] [--only heaviside|checkpoint|wcycle|control]``
+``python make_golden.py [REF_ROOT] [--only heaviside|checkpoint|wcycle|control|resume]``
 regenerates all fixtures, or only the named group.
 """
 
@@ -233,7 +235,28 @@ def main(ref_root: str) -> None:
     checkpoint_fixtures(ref_root)
     wcycle_fixtures(ref_root)
     control_fixtures(ref_root)
+    resume_fixtures(ref_root)
     print("golden fixtures written to", HERE)
+
+
+def resume_fixtures(ref_root) -> None:
+    import tempfile
+
+    _setup(Path(ref_root))
+    from gpu_fem.pub_simp_solver import SIMPParams, run_simp
+
+    d = {}
+    with tempfile.TemporaryDirectory() as tmp:
+        for leg, max_iter in (("a", 4), ("b", 7)):
+            params = SIMPParams(nelx=16, nely=8, nelz=4, volfrac=0.3, rmin=1.5, move=0.2, max_iter=max_iter,
+                                min_iter=max_iter, use_heaviside=True, beta_init=2.0, checkpoint_dir=tmp,
+                                checkpoint_every=2)
+            with redirect_stdout(io.StringIO()):
+                res = run_simp(params, verbose=False)
+            d[f"compliance_{leg}"] = np.array(res["compliance_history"])
+            d[f"rho_final_{leg}"] = res["rho_final"]
+            d[f"n_iter_{leg}"] = np.array(res["n_iter"])
+    np.savez_compressed(HERE / "run_simp_resume.npz", **d)
 
 
 class ScriptedController:
@@ -351,7 +374,7 @@ if __name__ == "__main__":
 
     ap = argparse.ArgumentParser()
     ap.add_argument("ref_root", nargs="?", default="/root/reference")
-    ap.add_argument("--only", choices=["heaviside", "checkpoint", "wcycle", "control"], default=None)
+    ap.add_argument("--only", choices=["heaviside", "checkpoint", "wcycle", "control", "resume"], default=None)
     a = ap.parse_args()
     if a.only == "heaviside":
         heaviside_fixtures(a.ref_root)
@@ -361,5 +384,7 @@ if __name__ == "__main__":
         wcycle_fixtures(a.ref_root)
     elif a.only == "control":
         control_fixtures(a.ref_root)
+    elif a.only == "resume":
+        resume_fixtures(a.ref_root)
     else:
         main(a.ref_root)

@@ -187,3 +187,26 @@ def test_simpsolver_cpu_backend_runs_run_simp_on_device(cuda_dev):
     np.testing.assert_allclose([r["compliance"] for r in res.history], ref["compliance_history"], rtol=1e-6)
     assert res.summary["backend"] == "cpu" and res.summary["n_iter"] == ref["n_iter"]
     np.testing.assert_allclose(res.rho_final, ref["rho_final"], atol=1e-5)
+
+
+def test_driver_checkpoint_resume_matches_reference(tmp_path):
+    """Interrupted after 4 of 7 iterations (checkpoint_every 2) and resumed,
+    as the reference run_simp did for ``run_simp_resume.npz``: both legs with
+    the oracle physics, and the second leg really starts from the checkpoint."""
+    from topogpu_b200.run_simp import SIMPParams, cantilever_bc_3d, run_simp
+
+    g = load_golden("run_simp_resume")
+    _, free, F = cantilever_bc_3d(16, 8, 4)
+    for leg, max_iter in (("a", 4), ("b", 7)):
+        fea = OracleFEA((16, 8, 4), free, F)
+        calls = []
+        step = fea.step
+        fea.step = lambda *a, _s=step, _c=calls: (_c.append(1), _s(*a))[1]
+        p = SIMPParams(nelx=16, nely=8, nelz=4, volfrac=0.3, rmin=1.5, move=0.2, max_iter=max_iter,
+                       min_iter=max_iter, use_heaviside=True, beta_init=2.0, checkpoint_dir=str(tmp_path),
+                       checkpoint_every=2)
+        res = run_simp(p, fea=fea)
+        np.testing.assert_allclose(res["compliance_history"], g[f"compliance_{leg}"], rtol=1e-9)
+        np.testing.assert_allclose(res["rho_final"], g[f"rho_final_{leg}"], rtol=1e-7, atol=1e-9)
+        assert res["n_iter"] == int(g[f"n_iter_{leg}"])
+        assert len(calls) == (4 if leg == "a" else 3) + 1  # iterations run here + the final evaluation
