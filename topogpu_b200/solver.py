@@ -8,9 +8,9 @@ GMG setup, Krylov solve, compliance, sensitivity and the bisection OC update
 that go into the history rows.
 
 Defaults reproduce the reference path: no density filter, penalty 3,
-OC on the plain mean volume. ``backend="cpu"`` (the reference's CPU
-backend, ``run_simp``) runs that driver with its physics on the GPU
-(``topogpu_b200.run_simp``). ``use_filter=True`` switches to the filtered
+OC on the plain mean volume. ``backend="cpu"`` (the default, as in the
+reference: its CPU backend, ``run_simp``) runs that driver with its physics
+on the GPU (``topogpu_b200.run_simp``). ``use_filter=True`` switches to the filtered
 formulation of the reference's CPU driver ``run_simp``
 (src/gpu_fem/pub_simp_solver.py:342-377): physical density H rho,
 sensitivities chained through H^T, volume measured after the filter.
@@ -86,7 +86,7 @@ class SIMPSolver:
     default, "w": SolverV4's gmg_cycle_type), device.
     """
 
-    def __init__(self, backend="cuda", linear_solver="auto", optimizer="oc", tol=1.0e-5, max_krylov=800,
+    def __init__(self, backend="cpu", linear_solver="auto", optimizer="oc", tol=1.0e-5, max_krylov=800,
                  max_iter=12, move=0.10, rho_min=1.0e-3, *, precision="mixed", levels=4, fine_degree=2,
                  coarse_degree=2, use_filter=False, use_heaviside=False, beta=1.0, eta=0.5, penal=3.0,
                  smoother="chebyshev", coarse_lag=None, checkpoint_dir=None, checkpoint_every=10,
