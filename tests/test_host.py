@@ -38,6 +38,30 @@ def test_library_reports_errors_without_gpu_work():
     assert "grid dims" in _lib.last_error(None)
 
 
+def test_entries_reject_a_null_context_without_gpu_work():
+    """Every context entry validates its arguments before touching the device:
+    a NULL context is an error status naming the entry (the byte-count query
+    answers 0)."""
+    from topogpu_b200 import _lib
+
+    lib = _lib.load()
+    no_ctx = {"topo_version", "topo_last_error", "topo_ctx_destroy", "topo_launch_count", "topo_ctx_create",
+              "topo_oc_noalloc"}
+    checked = 0
+    for name, (restype, argtypes) in sorted(_lib.SIGNATURES.items()):
+        if name in no_ctx:
+            continue
+        args = [t() if t is not ctypes.c_void_p else None for t in argtypes]
+        rc = getattr(lib, name)(*args)
+        if name == "topo_workspace_bytes":
+            assert rc == 0
+            continue
+        assert rc < 0, name
+        assert name in _lib.last_error(None), (name, _lib.last_error(None))
+        checked += 1
+    assert checked >= 25
+
+
 def test_product_stiffness_matches_reference():
     from topogpu_b200.fem import KE_UNIT
 
