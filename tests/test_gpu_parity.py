@@ -469,4 +469,38 @@ def test_different_element_stiffness_refused_while_shared_one_is_live(cuda_dev):
     with pytest.raises(RuntimeError, match="different element stiffness"):
         TopoContext((4, 2, 2), n_levels=1, mode="fp64", KE=KE_UNIT * 2.0)
     b = TopoContext((4, 2, 2), n_levels=1, mode="fp64", KE=KE_UNIT.copy())
-    assert a.ndof == b.ndof
+    # the reference's KE_UNIT_3D differs from this one in the last bits: same stiffness
+    c = TopoContext((4, 2, 2), n_levels=1, mode="fp64", KE=load_golden("ke_edof")["KE"])
+    assert a.ndof == b.ndof == c.ndof
+
+
+def test_solverv4_class_matches_reference_fixture(cuda_dev):
+    """tg.SolverV4 built with the reference's own constructor arguments
+    (solver_v4.py:38-145, as in the solverv4.npz generator, with the
+    reference's KE_UNIT_3D) and driven by the host OC: the reference's
+    compliances to 1e-9 and densities to 1e-7."""
+    import topogpu_b200 as tg
+
+    g = load_golden("solverv4")
+    ke = load_golden("ke_edof")["KE"]
+    nel = (24, 12, 6)
+    bc = fem.cantilever_bc(nel)
+    s = tg.SolverV4(edof=None, row_idx=None, col_idx=None, KE_UNIT=ke, free=bc.free.astype(np.int32), F=bc.F,
+                    ndof=bc.ndof, backend="cupy", enable_warm_start=True, enable_matrix_free=True,
+                    enable_fused_cuda=False, enable_matfree_gmg=True, matfree_gmg_levels=4,
+                    gmg_fine_smoother="fp64", gmg_smoother_type="chebyshev", grid_dims=nel, cg_tol=1e-8,
+                    cg_maxiter=800, enable_profiling=True)
+    rho = np.full(1728, 0.3)
+    comps = []
+    for k in range(3):
+        c, dc = s.solve(rho, penal=3.0)
+        comps.append(c)
+        # PCG on this 131-iteration case is not reproducible to the iteration
+        # (the reference V-cycle is only nearly symmetric): within 5%
+        assert isinstance(dc, np.ndarray) and abs(s.last_cg_iters - int(g["iters_fp64"][k])) <= 0.05 * int(
+            g["iters_fp64"][k]) + 1
+        rho, _ = design.oc_update(rho, dc, 0.3, 0.2)
+        assert np.max(np.abs(rho - g["rho_fp64"][k])) < 1e-7
+    np.testing.assert_allclose(comps, g["compliance_fp64"], rtol=1e-9)
+    assert s.last_outer_solver == "pcg" and s.last_timing
+    s.close()

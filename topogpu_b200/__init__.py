@@ -27,6 +27,7 @@ _EXPORTS = {
     "MatrixFreeOperator": ("topogpu_b200.operators", "MatrixFreeOperator"),
     "GMGPreconditioner": ("topogpu_b200.operators", "GMGPreconditioner"),
     "StateSolver": ("topogpu_b200.state", "StateSolver"),
+    "SolverV4": ("topogpu_b200.solver_v4", "SolverV4"),
     "run_simp": ("topogpu_b200.run_simp", "run_simp"),
     "SIMPParams": ("topogpu_b200.run_simp", "SIMPParams"),
     "StepState": ("topogpu_b200.run_simp", "StepState"),

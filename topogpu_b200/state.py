@@ -30,14 +30,14 @@ class StateSolver:
     def __init__(self, nel, free_mask, F, *, n_levels=4, precision="mixed", fine_degree=2, coarse_degree=2,
                  cheb_lower=1.0 / 30.0, outer="pcg", restart=32, tol=1e-5, maxiter=800, warm_start=True,
                  E0=1.0, Emin=1e-9, dense_max=16384, smoother="chebyshev", probe=False, cycle_type="v",
-                 device=None):
+                 KE=None, device=None):
         if outer not in ("pcg", "fgmres"):
             raise ValueError(f"outer must be 'pcg' or 'fgmres', got {outer!r}")
         self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
         with torch.cuda.device(self.device):
             self.ctx = TopoContext(nel, n_levels=n_levels, mode=precision, fine_degree=fine_degree,
                                    coarse_degree=coarse_degree, cheb_lower=cheb_lower, dense_max=dense_max,
-                                   smoother=smoother)
+                                   KE=KE, smoother=smoother)
         self.ctx.set_cycle(cycle_type)
         self.cycle_type = cycle_type
         self.nel = self.ctx.nel
