@@ -29,7 +29,6 @@ import torch
 
 from .checkpoint import checkpoint_path, load_checkpoint, save_checkpoint
 
-E0, EMIN = 1.0, 1e-9
 MIN_ITER_FOR_FALLBACK = 10  # pub_simp_solver.py:488
 
 
