@@ -131,6 +131,9 @@ def test_density_filter_host_api():
                                rtol=1e-15)
     w = tg.DensityFilter((3, 2, 2), radius=1.5).matrix()
     assert np.allclose(w.sum(axis=1), 1.0, atol=1e-12)
+    # the energy form of the reference's tests/test_energy_consistency.py
+    rho = np.linspace(0.1, 1.0, w.shape[0])
+    assert float(rho @ (w @ rho)) > 0.0
 
 
 def test_evidence_bundle_manifest(tmp_path):
