@@ -43,6 +43,22 @@ MICRO_NEL = (192, 96, 48)
 FALLBACK_PEAKS = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
 
 
+def traffic_for(name: str):
+    """DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of
+    a kernel from its committed ncu summary, used only when that capture was
+    taken with the library being run (same SHA-256), else None."""
+    import hashlib
+
+    f = ROOT / "profiles" / f"{name}_traffic.json"
+    lib = ROOT / "topogpu_b200" / "libtopo_b200.so"
+    if not f.exists() or not lib.exists():
+        return None
+    d = json.loads(f.read_text())
+    if d.get("lib_sha256") != hashlib.sha256(lib.read_bytes()).hexdigest():
+        return None
+    return d.get("bytes_per_launch")
+
+
 def peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -97,9 +113,20 @@ class Clocks:
                 "samples": len(sm)}
 
 
+def _rel_l2(a, b):
+    a, b = a.double(), b.double()
+    return float(torch.linalg.vector_norm(a - b) / torch.linalg.vector_norm(b))
+
+
 def ku_micro(reps: int = 100, pairs: int = 8):
     """Level-0 K.u on the 192x96x48 grid: FP64, FP32 and BF16-input, with
-    rotating buffers (> L2). Returns per-precision GDoF/s, bytes and times."""
+    rotating buffers (> L2). Returns per-precision GDoF/s, algorithmic bytes,
+    times, launch counts and the relative L2 error of the FP32 and BF16
+    operators against FP64 on the same u and E. Algorithmic bytes per launch:
+    ndof*(s_u + s_y) + nelem*s_E (structured element map computed, vectors
+    read or written once); the reference's 340 B/element model
+    (experiments/paper4/run_experiments_e1_e10.py:659-660) is reported beside
+    it, labelled as that model."""
     from topogpu_b200.bc import cantilever_edge_load
     from topogpu_b200.context import TopoContext
 
@@ -113,14 +140,18 @@ def ku_micro(reps: int = 100, pairs: int = 8):
     E64 = (1e-9 + (1 - 1e-9) * rho ** 3).to(dev)
     out = {}
     ndof, ne = ctx.ndof, ctx.n_elem
+    base = [(torch.randn(ndof, generator=g, dtype=torch.float64) * torch.tensor(mask, dtype=torch.float64)).to(dev)
+            for _ in range(pairs)]
+    first = {}
     for name, dt in (("fp64", torch.float64), ("fp32", torch.float32), ("bf16", torch.bfloat16)):
         Edt = torch.float64 if dt == torch.float64 else torch.float32
         E = E64.to(Edt)
-        us = [(torch.randn(ndof, generator=g) * mask.astype(np.float32)).to(dev).to(dt) for _ in range(pairs)]
+        us = [b.to(dt) for b in base]
         ys = [torch.empty(ndof, dtype=Edt, device=dev) for _ in range(pairs)]
         for k in range(3):
             ctx.matvec(us[k % pairs], E, out=ys[k % pairs])
         torch.cuda.synchronize()
+        first[name] = ctx.matvec(us[0], E).clone()
         n0 = ctx._lib.topo_launch_count()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
@@ -133,9 +164,62 @@ def ku_micro(reps: int = 100, pairs: int = 8):
         s_y = 8 if name == "fp64" else 4
         byts = ndof * (s_u + s_y) + ne * (8 if name == "fp64" else 4)
         out[name] = {"ms": ms, "gdof_s": ndof / (ms * 1e-3) / 1e9, "bytes": byts, "gbs": byts / (ms * 1e-3) / 1e9,
-                     "gflops": 1152 * ne / (ms * 1e-3) / 1e9, "launches": int(ctx._lib.topo_launch_count() - n0)}
+                     "gflops": 1152 * ne / (ms * 1e-3) / 1e9,
+                     "ref_model_gbs": 340.0 * ne / (ms * 1e-3) / 1e9,
+                     "launches_per_apply": (ctx._lib.topo_launch_count() - n0) / reps}
+    out["fp32"]["rel_l2_vs_fp64"] = _rel_l2(first["fp32"], first["fp64"])
+    out["bf16"]["rel_l2_vs_fp64"] = _rel_l2(first["bf16"], first["fp64"])
+    out["kernels"] = {"fp64": "k_level0<double> (CUDA cores)", "fp32": "k_level0<float> (CUDA cores)",
+                      "bf16": "k_level0_xs<bf16, Store> (tcgen05, BF16 u, TMA-staged x-planes)"}
     ctx.close()
     return out
+
+
+def cheb_micro(reps: int = 30, sets: int = 3):
+    """The Chebyshev step the mixed smoother runs on level 0, alone: the
+    tensor-core K.u with FP32 u rounded to BF16 when staged and the fused
+    epilogue r -= s K u; d = c1 u + c2 dinv r; x += ax d, on the 160x80x80
+    SIMP mesh with `sets` rotating vector sets (> L2). Algorithmic bytes per
+    launch: ndof*(4 u + 8 r + 4 dinv + 8 x + 4 d) + nelem*4 E."""
+    from topogpu_b200.bc import cantilever_edge_load
+    from topogpu_b200.context import TopoContext
+
+    dev = torch.device("cuda", torch.cuda.current_device())
+    ctx = TopoContext(NEL, n_levels=1, mode="mixed")
+    mask, F = cantilever_edge_load(NEL)
+    ctx.set_problem(torch.tensor(mask, device=dev), torch.tensor(F, device=dev))
+    g = torch.Generator(device="cpu").manual_seed(2)
+    rho = torch.rand(ctx.n_elem, generator=g, dtype=torch.float64) * 0.999 + 0.001
+    E = (1e-9 + (1 - 1e-9) * rho ** 3).float().to(dev)
+    m = torch.tensor(mask, dtype=torch.float32, device=dev)
+    nd, ne = ctx.ndof, ctx.n_elem
+
+    def vec():
+        return torch.randn(nd, generator=g).to(dev) * m
+
+    S = [dict(u=vec(), r=vec(), x=vec(), d=torch.zeros(nd, device=dev), dinv=(torch.rand(nd, generator=g).to(dev) + 0.1) * m)
+         for _ in range(sets)]
+
+    def run(k):
+        v = S[k % sets]
+        ctx.level0_apply(v["u"], E, "cheb", r=v["r"], x=v["x"], d_out=v["d"], dinv=v["dinv"], s=0.5, c1=0.3, c2=0.9,
+                         ax=1.0, u_fp32_to_bf16=True)
+
+    for k in range(3):
+        run(k)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for k in range(reps):
+        run(k)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    byts = nd * 28 + ne * 4
+    ctx.close()
+    return {"kernel": "k_level0_xs<float, ChebR> (tcgen05, FP32 u rounded to BF16, fused Chebyshev epilogue)",
+            "workload": "160x80x80 hex8 (3,168,963 DoF), 3 rotating vector sets", "ms": ms, "bytes": byts,
+            "gbs": byts / (ms * 1e-3) / 1e9, "gdof_s": nd / (ms * 1e-3) / 1e9}
 
 
 def simp_steps(precision, steps, warmup, flush, rmin=2.0):
@@ -222,30 +306,57 @@ def fp64_compliance_check(rho_first=0.30, rmin=2.0):
     return abs(out["mixed"] - out["fp64"]) / abs(out["fp64"])
 
 
-def cpu_baseline(sample_nel=(48, 24, 24), steps=3):
-    """The CPU oracle (restated reference SolverV4 GMG-PCG with its default
-    FP32 smoother, filtered OC) on a reduced cantilever, scaled to 1M
-    elements by element count."""
+REF_SAMPLES = ((24, 12, 12), (48, 24, 24))
+
+
+def _oracle_step_seconds(nel, steps):
+    """Seconds per filtered SIMP iteration of the CPU oracle (the restated
+    reference SolverV4 GMG-PCG: FP64 PCG, FP32 Chebyshev smoother, degree 3,
+    4 levels, rtol 1e-5; filter rmin 2.0, move 0.2) on an nel cantilever,
+    averaged over `steps` iterations from the uniform start."""
     from oracle import fem, simp
 
-    bc = fem.cantilever_bc(sample_nel)
-    s = simp.FilteredSIMP(sample_nel, bc, 0.30, 2.0, move=0.2, n_levels=4, fine_prec="fp32", fine_degree=3,
-                          tol=1e-5, maxiter=800)
+    bc = fem.cantilever_bc(nel)
+    s = simp.FilteredSIMP(nel, bc, 0.30, 2.0, move=0.2, n_levels=4, fine_prec="fp32", fine_degree=3, tol=1e-5,
+                          maxiter=800)
     t0 = time.perf_counter()
     its = []
     for _ in range(steps):
         s.step()
         its.append(s.state.last_iters)
-    dt = time.perf_counter() - t0
-    ne = int(np.prod(sample_nel))
-    scale = ne / float(np.prod(NEL))
-    rate = steps / dt * scale
+    return (time.perf_counter() - t0) / steps, its
+
+
+def oracle_scaling(steps=2):
+    """Measured size law of the oracle SIMP iteration: t(n) = t(n1) (n/n1)^a
+    from two sample meshes, a fitted on them, used to carry the larger
+    sample to the 1,024,000-element mesh (which takes minutes per iteration
+    on the host and does not fit the benchmark's time box)."""
+    (n1, n2) = (int(np.prod(REF_SAMPLES[0])), int(np.prod(REF_SAMPLES[1])))
+    t1, it1 = _oracle_step_seconds(REF_SAMPLES[0], steps)
+    t2, it2 = _oracle_step_seconds(REF_SAMPLES[1], steps)
+    a = float(np.log(t2 / t1) / np.log(n2 / n1))
+    return {"t_small_s": t1, "t_large_s": t2, "exponent": a, "its_small": it1, "its_large": it2, "n_small": n1,
+            "n_large": n2}
+
+
+def scale_to_full(t_large_s, law):
+    return t_large_s * (float(np.prod(NEL)) / law["n_large"]) ** law["exponent"]
+
+
+def cpu_baseline(steps=2):
+    """The CPU oracle's SIMP iteration rate at 160x80x80 from the measured
+    size law (bounded sample: two iterations at each of two sample meshes)."""
+    law = oracle_scaling(steps)
+    t_full = scale_to_full(law["t_large_s"], law)
     cores = len(os.sched_getaffinity(0))
-    return {"value": rate, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": (f"{steps} filtered SIMP iterations of the oracle (reference SolverV4 GMG-PCG, FP32 smoother, "
-                       f"deg 3, 4 levels, rtol 1e-5; PCG its {its}) on the {'x'.join(map(str, sample_nel))} "
-                       f"cantilever ({ne} elements) in {dt:.1f} s on {cores} host cores (NumPy/SciPy threads), "
-                       f"rate scaled to 1,024,000 elements by element count")}
+    return {"value": 1.0 / t_full, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": (f"{steps} filtered SIMP iterations of the CPU oracle (restated reference SolverV4 GMG-PCG, FP64 "
+                       f"PCG, FP32 smoother deg 3, 4 levels, rtol 1e-5) on each of "
+                       f"{'x'.join(map(str, REF_SAMPLES[0]))} ({law['t_small_s']:.2f} s/it, PCG its {law['its_small']}) and "
+                       f"{'x'.join(map(str, REF_SAMPLES[1]))} ({law['t_large_s']:.2f} s/it, PCG its {law['its_large']}); "
+                       f"measured law t ~ n^{law['exponent']:.2f} carries the larger to 1,024,000 elements; "
+                       f"{cores} host cores (NumPy/SciPy threads)")}
 
 
 def max_over_ranks(x: float, dist, device="cuda") -> float:
@@ -308,35 +419,42 @@ def extras():
 
 
 def reference_arm(args, rank):
+    """The reference's algorithm on the host cores (the CPU oracle: the
+    reference is Python on CuPy, which is not installed, so it cannot run
+    on the GPU box itself). Warm-up calibrates the size law on two sample
+    meshes; each timed step is one SIMP iteration on the larger sample,
+    carried to 160x80x80 by that law."""
     if rank != 0:
         return 0
     os.environ.setdefault("OMP_NUM_THREADS", str(len(os.sched_getaffinity(0))))
     from oracle import fem, simp
 
-    nel = (48, 24, 24)
+    law = oracle_scaling(steps=max(1, min(args.warmup, 2)))
+    nel = REF_SAMPLES[1]
     bc = fem.cantilever_bc(nel)
     s = simp.FilteredSIMP(nel, bc, 0.30, 2.0, move=0.2, n_levels=4, fine_prec="fp32", fine_degree=3, tol=1e-5,
                           maxiter=800)
-    for _ in range(args.warmup):
-        s.step()
-    times = []
+    times, its = [], []
     for _ in range(args.steps):
         t0 = time.perf_counter()
         s.step()
         times.append(time.perf_counter() - t0)
-    scale = float(np.prod(nel)) / float(np.prod(NEL))
-    ms = statistics.mean(times) * 1e3 / scale
+        its.append(s.state.last_iters)
+    t_full = scale_to_full(statistics.mean(times), law)
+    ms = t_full * 1e3
     value = 1e3 / ms
     cores = len(os.sched_getaffinity(0))
+    sample = (f"one SIMP iteration per step of the CPU oracle (restated reference SolverV4 GMG-PCG: FP64 PCG, FP32 "
+              f"Chebyshev smoother deg 3, 4 levels, rtol 1e-5, filter rmin 2.0) on "
+              f"{'x'.join(map(str, nel))} ({law['n_large']} hex, PCG its {its}), carried to 1,024,000 hex by the "
+              f"law t ~ n^{law['exponent']:.2f} measured in warm-up on "
+              f"{'x'.join(map(str, REF_SAMPLES[0]))} and {'x'.join(map(str, REF_SAMPLES[1]))}")
     line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64 PCG / f32 smoother", "data": "synthetic",
             "config": {"workload": "cantilever 160x80x80 (1,024,000 hex) filtered SIMP, GMG-PCG rtol 1e-5",
-                       "sample": "48x24x24 (27,648 hex) per step, rate scaled by element count",
-                       "parallelism": "host CPU"},
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
-                             "sample": "one SIMP iteration of the CPU oracle (restated reference SolverV4 "
-                                       "GMG-PCG, FP32 smoother) on 48x24x24 per step, scaled by element count"},
+                       "sample": sample, "parallelism": "host CPU"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
@@ -377,7 +495,7 @@ def main():
     flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
     if args.only_ku:
-        print(json.dumps({"ku": ku_micro(args.micro_reps)}))
+        print(json.dumps({"ku": ku_micro(args.micro_reps), "cheb": cheb_micro()}))
         return 0
     if args.only_simp:
         r = simp_steps("mixed", args.steps, args.warmup, flush)
@@ -406,14 +524,16 @@ def main():
 
     pk = peaks()
     b = micro["bf16"]
-    roof = {"kernel": "tc::k_level0_tc<float, Store> (level-0 K.u, tcgen05 BF16 input, FP32 accumulate in TMEM)",
+    roof = {"kernel": micro["kernels"]["bf16"] + ", level-0 K.u y = K(E) u",
             "workload": "192x96x48 hex8 (2,751,987 DoF), 8 rotating (u,y) pairs", "bound": "hbm",
             "achieved": b["gbs"], "peak": pk["hbm_gbs"], "unit": "GB/s", "frac": b["gbs"] / pk["hbm_gbs"],
-            "traffic": None, "peak_source": pk["source"], "bytes_per_launch": b["bytes"],
-            "launch_ms": b["ms"]}
-    tr = ROOT / "profiles" / "k_level0_tc_192x96x48_traffic.json"
-    if tr.exists():
-        roof["traffic"] = json.loads(tr.read_text()).get("bytes_per_launch")
+            "traffic": traffic_for("k_level0_xs_bf16_store_192x96x48"), "peak_source": pk["source"],
+            "bytes_per_launch": b["bytes"], "launch_ms": b["ms"]}
+    ch = cheb_micro()
+    roof_cheb = {"kernel": ch["kernel"], "workload": ch["workload"], "bound": "hbm", "achieved": ch["gbs"],
+                 "peak": pk["hbm_gbs"], "unit": "GB/s", "frac": ch["gbs"] / pk["hbm_gbs"],
+                 "traffic": traffic_for("k_level0_xs_float_cheb_160x80x80"), "peak_source": pk["source"],
+                 "bytes_per_launch": ch["bytes"], "launch_ms": ch["ms"]}
 
     iters = [r["outer_iters"] for r in mixed["rows"][args.warmup:]]
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -430,9 +550,9 @@ def main():
                 "value": world * 1e3 / (sum(fp32["ms"]) / args.steps), "ms_per_step": sum(fp32["ms"]) / args.steps,
                 "pcg_iters_per_step": [r["outer_iters"] for r in fp32["rows"][args.warmup:]],
                 "step_breakdown_ms": fp32["breakdown"]},
-            "ku": {k: {"gdof_s": v["gdof_s"], "gbs": v["gbs"], "ms": v["ms"], "gflops": v["gflops"]}
-                   for k, v in micro.items()},
+            "ku": {k: v for k, v in micro.items()},
             "roofline": roof,
+            "roofline_cheb_step": roof_cheb,
             "clocks": clk,
             "gpu_launches": launches,
             "e2e": {"value": replica_rate(world, e2e_ms / args.steps), "unit": UNIT,

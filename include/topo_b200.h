@@ -30,8 +30,12 @@ extern "C" {
 
 typedef struct topo_ctx topo_ctx;
 
-/* Arithmetic of a vector or operator. */
-enum { TOPO_F64 = 0, TOPO_F32 = 1, TOPO_BF16 = 2 };
+/* Arithmetic of a vector or operator. TOPO_BF16_F32IN: BF16 operator whose
+ * input u is stored FP32 and rounded to BF16 when staged (the smoother's form). */
+enum { TOPO_F64 = 0, TOPO_F32 = 1, TOPO_BF16 = 2, TOPO_BF16_F32IN = 3 };
+
+/* Epilogues of the level-0 operator (topo_level0_apply). */
+enum { TOPO_EPI_STORE = 0, TOPO_EPI_RESIDUAL = 1, TOPO_EPI_CHEB = 2, TOPO_EPI_RUPD = 4 };
 
 /* Precision schedule of the state solve.
  *  FP64  : FP64 outer PCG, FP64 operators on every level.
@@ -100,6 +104,33 @@ int topo_modulus(topo_ctx* ctx, const double* rho, double penal, double E0, doub
  *  BF16-rounded u and KE accumulated in FP32 on the tensor cores. */
 int topo_matvec(topo_ctx* ctx, int dtype, const void* u, void* y, const void* E, void* stream);
 
+/* Level-0 operator with its fused epilogue: the building block of the
+ * smoother, exposed so each form can be checked on its own.
+ *  u_dtype TOPO_F64: FP64 CUDA cores; u, E and the epilogue vectors double.
+ *          TOPO_F32: FP32 CUDA cores; everything float.
+ *          TOPO_BF16 / TOPO_BF16_F32IN: tensor cores, u bf16 / float, E and
+ *          the epilogue vectors float.
+ *  epi TOPO_EPI_STORE    y = K u
+ *      TOPO_EPI_RESIDUAL y = b - K u
+ *      TOPO_EPI_RUPD     r = r - s K u
+ *      TOPO_EPI_CHEB     r = r - s K u; d_out = c1 u + c2 dinv r; x = x + ax d_out
+ * Fixed DoFs of y, r and d_out are set to zero (x keeps them). u and d_out
+ * must differ; r and x are updated in place. Every vector 16-byte aligned.
+ * Replaces one step of the fused smoother _chebyshev_steps / _smooth_fine
+ * (src/gpu_fem/multigrid_v4.py:861-932) over FusedMatvec.matvec
+ * (src/gpu_fem/cuda_fused_matvec.py:336-370). */
+int topo_level0_apply(topo_ctx* ctx, int u_dtype, int epi, const void* u, const void* E, void* y, const void* b,
+                      void* r, void* x, void* d_out, const void* dinv, double s, double c1, double c2, double ax,
+                      void* stream);
+
+/* Test hook for the bounded waits of the tensor-core K.u (no reference
+ * counterpart): with skip_first_arrival != 0 the kernel's converter warps
+ * withhold their first arrival, so its MMA role's wait runs out after
+ * poll_limit polls (<= 0: the default limit); the kernel then raises its
+ * error flag, drains and exits, and the entry point that launched it
+ * returns an error. Applies to later launches in this process. */
+int topo_debug_tc_wait(int skip_first_arrival, int poll_limit);
+
 /* diag(K(E)) on all DoFs (zero at fixed DoFs).
  * Replaces MatrixFreeKff.extract_diagonal (src/gpu_fem/solver_v2.py:1229-1252). */
 int topo_diag(topo_ctx* ctx, const double* E, double* diag, void* stream);
@@ -133,6 +164,19 @@ int topo_pcg(topo_ctx* ctx, const void* b, void* x, double tol, int maxiter, int
 int topo_fgmres(topo_ctx* ctx, const void* b, void* x, double tol, int maxiter, int restart,
                 int* out_iters, double* out_relres, void* stream);
 
+/* Lagged coarsest factor (on != 0): from the second topo_gmg_setup on, the
+ * V-cycle applies the coarsest factor of the previous setup while the factor
+ * of the current operator is built on a background stream (it replaces the
+ * old one at the next setup). The preconditioner stays symmetric positive
+ * definite; Krylov solves still converge to their tolerance. Off by default;
+ * the reference refactorises synchronously (multigrid_v4.py:774-811). */
+int topo_set_coarse_lag(topo_ctx* ctx, int on);
+
+/* BF16 level-0 operator on the tensor cores (on != 0, the default) or on the
+ * CUDA cores (same BF16 inputs and FP32 accumulation, another summation
+ * order); a tuning switch with no reference counterpart. */
+int topo_set_tc(topo_ctx* ctx, int on);
+
 /* Block PCG for nrhs load cases (1..8) on the current hierarchy: B and X are
  * nrhs full-length FP64 vectors stored one after another (X holds the
  * initial guesses and receives the solutions). One multi-vector FP64 K.u per
@@ -142,19 +186,6 @@ int topo_fgmres(topo_ctx* ctx, const void* b, void* x, double tol, int maxiter, 
  * Returns 0 (all converged), 1 (maxiter reached) or < 0. The reference solves
  * one load case per PCG (_cupy_pcg, src/gpu_fem/solver_v2.py:552-624); this
  * replaces nrhs of those calls. */
-/* BF16 level-0 operator on the tensor cores (on != 0, the default) or on the
- * CUDA cores (same BF16 inputs and FP32 accumulation, another summation
- * order); a tuning switch with no reference counterpart. */
-/* Lagged coarsest factor (on != 0): from the second topo_gmg_setup on, the
- * V-cycle applies the coarsest factor of the previous setup while the factor
- * of the current operator is built on a background stream (it replaces the
- * old one at the next setup). The preconditioner stays symmetric positive
- * definite; Krylov solves still converge to their tolerance. Off by default;
- * the reference refactorises synchronously (multigrid_v4.py:774-811). */
-int topo_set_coarse_lag(topo_ctx* ctx, int on);
-
-int topo_set_tc(topo_ctx* ctx, int on);
-
 int topo_block_pcg(topo_ctx* ctx, const double* B, double* X, int nrhs, double tol, int maxiter,
                    int* out_iters, double* out_relres, void* stream);
 
@@ -224,7 +255,9 @@ int topo_oc_projected(topo_ctx* ctx, double rmin, const double* rho, const doubl
  * an application whose device memory belongs to its own pool (a framework
  * caching allocator, a Go/JVM runtime), or a latency-bound loop that cannot
  * afford the device-wide synchronisation cudaMalloc/cudaFree may cause.
- * rho, dc, out: n FP64 values in device memory owned by the caller.
+ * rho, dc, out: n FP64 values in device memory owned by the caller; out
+ * must not alias rho or dc (the kernels take all three as non-aliasing
+ * pointers; a call with out == rho or out == dc is rejected).
  * Limit: 1 <= n <= 8,388,608 elements; larger n is rejected with an error.
  * Working memory is a 33,024-byte static device array inside the library,
  * held by every GPU that loads it until the process exits and shared by all

@@ -46,7 +46,7 @@ def test_entries_reject_a_null_context_without_gpu_work():
 
     lib = _lib.load()
     no_ctx = {"topo_version", "topo_last_error", "topo_ctx_destroy", "topo_launch_count", "topo_ctx_create",
-              "topo_oc_noalloc"}
+              "topo_oc_noalloc", "topo_debug_tc_wait"}
     checked = 0
     for name, (restype, argtypes) in sorted(_lib.SIGNATURES.items()):
         if name in no_ctx:

@@ -45,6 +45,7 @@ def test_no_alloc_rejects_sizes_beyond_its_scratch():
 def test_no_alloc_oc_matches_context_oc_twice(cuda_dev):
     import torch
 
+    from oracle import design
     from topogpu_b200 import _lib
     from topogpu_b200.context import TopoContext
 
@@ -52,17 +53,46 @@ def test_no_alloc_oc_matches_context_oc_twice(cuda_dev):
     g = load_golden("oc")
     rng = np.random.default_rng(12)
     n_big = 300_000
-    cases = [(g["rho_0"], g["dc_0"], float(g["vf_0"]), float(g["move_0"])),
-             (rng.uniform(0.001, 1.0, n_big), -rng.gamma(1.0, 1.0, n_big) * 10.0 ** rng.uniform(-4, 1, n_big), 0.3,
-              0.2)]
-    for rho_np, dc_np, vf, mv in cases:
+    # the reference's three OC fixtures, then a 300,000-element seeded case
+    cases = [(g[f"rho_{k}"], g[f"dc_{k}"], float(g[f"vf_{k}"]), float(g[f"move_{k}"]), g[f"out_{k}"]) for k in range(3)]
+    cases.append((rng.uniform(0.001, 1.0, n_big), -rng.gamma(1.0, 1.0, n_big) * 10.0 ** rng.uniform(-4, 1, n_big), 0.3,
+                  0.2, None))
+    for rho_np, dc_np, vf, mv, want in cases:
         rho = torch.tensor(rho_np, dtype=torch.float64, device=cuda_dev)
         dc = torch.tensor(dc_np, dtype=torch.float64, device=cuda_dev)
         ctx = TopoContext((rho.numel(), 1, 1), n_levels=1, mode="fp64")
         ref, ev_ref = ctx.oc(rho, dc, vf, mv)
+        _, ev_oracle = design.oc_update(rho_np, dc_np, vf, mv)
         for _ in range(2):  # two calls in a row share (and must clear) the static scratch
             rc, out, ev = _noalloc(lib, rho, dc, vf, mv)
             assert rc == 0, _lib.last_error(None)
             assert torch.equal(out, ref)
-            assert ev == ev_ref
+            assert ev == ev_ref == ev_oracle
+            if want is not None:
+                assert np.array_equal(out.cpu().numpy(), want)
         ctx.close()
+
+
+@pytest.mark.gpu
+def test_no_alloc_oc_at_its_size_limit(cuda_dev):
+    """n = 8,388,608 fills every partial-sum slot of the static scratch (the
+    slots just below the bisection state); the result must equal the
+    oracle's update bit for bit, twice in a row."""
+    import torch
+
+    from oracle import design
+    from topogpu_b200 import _lib
+
+    lib = _lib.load()
+    n = 8_388_608
+    rng = np.random.default_rng(21)
+    rho_np = rng.uniform(0.001, 1.0, n)
+    dc_np = -rng.gamma(1.0, 1.0, n) * 10.0 ** rng.uniform(-4, 1, n)
+    want, ev_want = design.oc_update(rho_np, dc_np, 0.4, 0.2)
+    rho = torch.tensor(rho_np, dtype=torch.float64, device=cuda_dev)
+    dc = torch.tensor(dc_np, dtype=torch.float64, device=cuda_dev)
+    for _ in range(2):
+        rc, out, ev = _noalloc(lib, rho, dc, 0.4, 0.2)
+        assert rc == 0, _lib.last_error(None)
+        assert ev == ev_want
+        assert np.array_equal(out.cpu().numpy(), want)

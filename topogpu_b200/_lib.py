@@ -12,7 +12,8 @@ from pathlib import Path
 _LIB_PATH = Path(__file__).resolve().parent / "libtopo_b200.so"
 _lib = None
 
-F64, F32, BF16 = 0, 1, 2
+F64, F32, BF16, BF16_F32IN = 0, 1, 2, 3
+EPI_STORE, EPI_RESIDUAL, EPI_CHEB, EPI_RUPD = 0, 1, 2, 4
 MODE_FP64, MODE_FP32, MODE_MIXED = 0, 1, 2
 MODES = {"fp64": MODE_FP64, "fp32": MODE_FP32, "mixed": MODE_MIXED}
 
@@ -31,6 +32,8 @@ SIGNATURES = {
     "topo_set_problem": (_i, [_vp, _vp, _vp, _vp]),
     "topo_modulus": (_i, [_vp, _vp, _d, _d, _d, _vp, _vp]),
     "topo_matvec": (_i, [_vp, _i, _vp, _vp, _vp, _vp]),
+    "topo_level0_apply": (_i, [_vp, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _d, _d, _d, _d, _vp]),
+    "topo_debug_tc_wait": (_i, [_i, _i]),
     "topo_diag": (_i, [_vp, _vp, _vp, _vp]),
     "topo_gmg_setup": (_i, [_vp, _vp, _vp]),
     "topo_gmg_apply": (_i, [_vp, _vp, _vp, _vp]),

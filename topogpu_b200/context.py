@@ -115,6 +115,41 @@ class TopoContext:
                                         _ptr(E, ydt, self.n_elem, "E"), _stream()), "matvec")
         return out
 
+    EPILOGUES = {"store": _lib.EPI_STORE, "residual": _lib.EPI_RESIDUAL, "rupd": _lib.EPI_RUPD,
+                 "cheb": _lib.EPI_CHEB}
+
+    def level0_apply(self, u, E, epi="store", *, y=None, b=None, r=None, x=None, d_out=None, dinv=None, s=1.0,
+                     c1=0.0, c2=0.0, ax=0.0, u_fp32_to_bf16=False):
+        """One level-0 operator application with its fused epilogue (see
+        topo_level0_apply): "store" y = K u, "residual" y = b - K u, "rupd"
+        r -= s K u, "cheb" r -= s K u; d_out = c1 u + c2 dinv r; x += ax d_out.
+        u's dtype picks the arithmetic (f64, f32, bf16); u_fp32_to_bf16 runs
+        an f32 u through the BF16 tensor-core operator (the smoother's form).
+        The other vectors are f64 for an f64 u and f32 otherwise. Returns y
+        for "store"/"residual", else None (r, x, d_out are updated)."""
+        if epi not in self.EPILOGUES:
+            raise ValueError(f"epi must be one of {sorted(self.EPILOGUES)}")
+        if u_fp32_to_bf16:
+            if u.dtype != torch.float32:
+                raise TypeError("u_fp32_to_bf16 needs an f32 u")
+            dt = _lib.BF16_F32IN
+        else:
+            dt = _DT.get(u.dtype)
+            if dt is None:
+                raise TypeError(f"unsupported dtype {u.dtype}")
+        vdt = torch.float64 if u.dtype == torch.float64 else torch.float32
+        if epi in ("store", "residual") and y is None:
+            y = torch.empty(self.ndof, dtype=vdt, device=u.device)
+
+        def opt(t, name, n=self.ndof):
+            return None if t is None else _ptr(t, vdt, n, name)
+
+        self._chk(self._lib.topo_level0_apply(self._h, dt, self.EPILOGUES[epi], _ptr(u, None, self.ndof, "u"),
+                                              _ptr(E, vdt, self.n_elem, "E"), opt(y, "y"), opt(b, "b"), opt(r, "r"),
+                                              opt(x, "x"), opt(d_out, "d_out"), opt(dinv, "dinv"), float(s), float(c1),
+                                              float(c2), float(ax), _stream()), "level0_apply")
+        return y if epi in ("store", "residual") else None
+
     def diag(self, E, out=None):
         out = torch.empty(self.ndof, dtype=torch.float64, device=E.device) if out is None else out
         self._chk(self._lib.topo_diag(self._h, _ptr(E, torch.float64, self.n_elem, "E"),

@@ -92,6 +92,12 @@ __global__ void k_gather_zero(long long n_full, T* __restrict__ x) {
     x[i] = 0;
 }
 
+// Per-node free bits from the per-DoF mask: bit c set <=> DoF 3n+c is free.
+__global__ void k_node_mask(long long nnodes, const uint8_t* __restrict__ mask, uint8_t* __restrict__ nmask) {
+  for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < nnodes; n += (long long)gridDim.x * blockDim.x)
+    nmask[n] = (uint8_t)((mask[3 * n] ? 1 : 0) | (mask[3 * n + 1] ? 2 : 0) | (mask[3 * n + 2] ? 4 : 0));
+}
+
 __global__ void k_add_diag(int n, double* A, double eps) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) A[(long long)i * n + i] += eps;
@@ -129,18 +135,10 @@ struct Level {
   int degree = 2;
 };
 
-// One factorisation of the coarsest operator and the graph that builds it.
+// One factorisation of the coarsest operator, with the stencil it is built from.
 struct FactorSlot {
-  int kind = 0;             // 0 none, 1 dense, 2 regularised dense
   double* S64c = nullptr;   // copy of the coarsest stencil the factor is built from
-  double* A = nullptr;      // assembled matrix, then the band of L
-  double* Dt = nullptr;     // factored diagonal blocks of L (32x32 each)
-  double* Di = nullptr;     // their inverses
-  double* work = nullptr;   // W = L^-1 (FP64); with FP64 vectors also W^T above the diagonal
-  float* X32 = nullptr;     // FP32 W / W^T apply matrix (FP32 vectors)
-  int* flag = nullptr;      // non-positive pivot seen
-  cudaGraphExec_t graph = nullptr;  // assembly + Cholesky + W, captured once
-  long long graph_kernels = 0;
+  CoarsestFactor f;
 };
 
 struct Coarsest {
@@ -148,8 +146,8 @@ struct Coarsest {
   int band = 0;
   int* dof_index = nullptr;
   int* free_list = nullptr;
-  long long ldc = 0;        // row stride of work / X32 (n rounded up to 32)
-  double* y = nullptr;      // compact FP64 intermediate of the two-pass apply
+  CoarsestPlan plan;
+  double* y = nullptr;      // 2n FP64: the forward and backward sweep vectors of the apply
   FactorSlot cur;           // the factor the V-cycle applies
   FactorSlot nxt;           // with coarse_lag: the factor being built in the background
   bool have = false;        // cur holds a factor
@@ -183,6 +181,7 @@ struct topo_ctx {
   Coarsest C;
   double* E64 = nullptr;
   float* E32 = nullptr;
+  uint8_t* nmask0 = nullptr;  // level 0: per-node free bits, bit c = DoF 3n+c (read by the tensor-core K.u)
   double* diag0 = nullptr;
   double lam_Emax = NAN;
   bool problem_set = false;
@@ -263,7 +262,8 @@ void op_apply(topo_ctx* c, int l, Prec p, const void* u, void* y, Epi epi, const
   Level& Lv = c->L[l];
   if (l == 0) {
     const void* E = (p == Prec::F64) ? (const void*)c->E64 : (const void*)c->E32;
-    if (p == Prec::BF16 && c->use_tc) level0_apply_tc(false, Lv.g, u, E, Lv.mask, y, epi, ea, s);
+    if (p == Prec::BF16 && c->use_tc && level0_xs_supported(Lv.g))
+      level0_apply_xs(false, Lv.g, u, E, c->nmask0, y, epi, ea, s);
     else level0_apply(p, Lv.g, u, E, Lv.mask, y, epi, ea, s);
   } else {
     const void* S = p == Prec::F64 ? (const void*)Lv.S64 : p == Prec::F32 ? (const void*)Lv.S32 : (const void*)Lv.S16;
@@ -320,7 +320,7 @@ void coarsest_solve(topo_ctx* c, const KrylovState* st, cudaStream_t s) {
   else k_gather_zero<float><<<gblocks(n_full), 256, 0, s>>>(n_full, (float*)Lv.x);
   TOPO_LAUNCH_CHECK();
   if (c->C.n == 0) return;
-  dense_apply(c->vec64, c->C.n, c->C.ldc, c->C.cur.work, c->C.cur.X32, c->C.free_list, Lv.b, c->C.y, Lv.x, st, s);
+  coarsest_apply(c->C.cur.f, c->vec64, Lv.b, c->C.y, Lv.x, st, s);
 }
 
 // One V-cycle (cycle_gamma 1, multigrid_v4.py:986-1008) or W-cycle
@@ -470,75 +470,42 @@ void host_galerkin_q(const double* KE, double* Q) {
 }
 
 // ------------------------------------------------ coarsest factorisation
+void* ctx_alloc_bytes(void* ctx, size_t bytes) {
+  return static_cast<void*>(static_cast<topo_ctx*>(ctx)->alloc<char>((long long)bytes));
+}
+
 void alloc_slot(topo_ctx* c, FactorSlot& f) {
-  const int n = c->C.n;
-  const long long nt = (n + 31) / 32;
-  if (f.graph) {
-    cudaGraphExecDestroy(f.graph);
-    f.graph = nullptr;
-  }
   f.S64c = c->alloc<double>(243LL * c->L[c->n_levels - 1].g.nnodes);
-  f.A = c->alloc<double>((long long)n * n);
-  f.Dt = c->alloc<double>(nt * 1024);
-  f.Di = c->alloc<double>(nt * 1024);
-  f.work = c->alloc<double>((long long)n * c->C.ldc);
-  f.X32 = c->vec64 ? nullptr : c->alloc<float>((long long)n * c->C.ldc);
-  f.flag = c->alloc<int>(1);
-  f.kind = 0;
+  coarsest_alloc(f.f, c->C.plan, c->C.band, c->vec64, ctx_alloc_bytes, c);
+  f.f.d_free = c->C.free_list;
+  f.f.kind = 0;
 }
 
-// Assembly (from the slot's stencil copy), banded Cholesky and W = L^-1 of
-// one slot, captured once as a graph: ~460 small launches become one.
-void slot_graph(topo_ctx* c, FactorSlot& f, cudaStream_t s) {
-  if (f.graph) return;
-  const Level& Lc = c->L[c->n_levels - 1];
-  const int n = c->C.n;
-  cudaGraph_t g;
-  const long long before = launch_count();
-  TOPO_CUDA_CHECK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-  dense_assemble(Lc.g, f.S64c, c->C.dof_index, n, f.A, s);
-  dense_cholesky_launch(n, c->C.band, f.A, f.Dt, f.flag, s);
-  dense_inverse_factor(n, c->C.band, f.A, f.Dt, f.Di, f.work, c->C.ldc, c->vec64 ? f.work : nullptr,
-                       c->vec64 ? nullptr : f.X32, s);
-  TOPO_CUDA_CHECK(cudaStreamEndCapture(s, &g));
-  f.graph_kernels = launch_count() - before;  // recorded, not launched: counted per replay
-  count_launches(-f.graph_kernels);
-  TOPO_CUDA_CHECK(cudaGraphInstantiate(&f.graph, g, 0));
-  TOPO_CUDA_CHECK(cudaGraphDestroy(g));
-}
-
+// Assembly (from the slot's stencil copy) and factorisation of one slot.
 void slot_launch(topo_ctx* c, FactorSlot& f, cudaStream_t s) {
-  slot_graph(c, f, s);
-  TOPO_CUDA_CHECK(cudaGraphLaunch(f.graph, s));
-  count_launches(f.graph_kernels);
+  const Level& Lc = c->L[c->n_levels - 1];
+  coarsest_assemble(f.f, Lc.g, f.S64c, c->C.dof_index, s);
+  coarsest_factor(f.f, s);
 }
 
-// After a slot's graph has run: read its pivot flag; on a non-positive pivot
-// rebuild it from the stencil copy with eps*I added (multigrid_v4.py:778-811).
+// After a slot's factorisation has run: read its pivot flag; on a
+// non-positive pivot rebuild it from the stencil copy with eps*I added
+// (multigrid_v4.py:778-811).
 void slot_finish(topo_ctx* c, FactorSlot& f, cudaStream_t s) {
-  int h = 0;
-  TOPO_CUDA_CHECK(cudaMemcpyAsync(&h, f.flag, sizeof(int), cudaMemcpyDeviceToHost, s));
-  TOPO_CUDA_CHECK(cudaStreamSynchronize(s));
-  if (!h) {
-    f.kind = 1;
+  const int st0 = coarsest_status(f.f, s);
+  if (st0 < 0) throw std::runtime_error("coarsest-level Cholesky: a grid barrier wait timed out");
+  if (st0 == 0) {
+    f.f.kind = 1;
     return;
   }
   const Level& Lc = c->L[c->n_levels - 1];
-  const int n = c->C.n;
-  dense_assemble(Lc.g, f.S64c, c->C.dof_index, n, f.A, s);
-  k_diag_sum<<<1, 256, 0, s>>>(n, f.A, c->dtmp);
-  TOPO_LAUNCH_CHECK();
-  double dsum;
-  TOPO_CUDA_CHECK(cudaMemcpyAsync(&dsum, c->dtmp, sizeof(double), cudaMemcpyDeviceToHost, s));
-  TOPO_CUDA_CHECK(cudaStreamSynchronize(s));
-  const double eps = std::max(dsum / n * 1e-8, 1e-14);
-  k_add_diag<<<(n + 255) / 256, 256, 0, s>>>(n, f.A, eps);
-  TOPO_LAUNCH_CHECK();
-  if (dense_cholesky(n, c->C.band, f.A, f.Dt, f.flag, s))
-    throw std::runtime_error("coarsest-level Cholesky failed even after eps*I regularisation");
-  dense_inverse_factor(n, c->C.band, f.A, f.Dt, f.Di, f.work, c->C.ldc, c->vec64 ? f.work : nullptr,
-                       c->vec64 ? nullptr : f.X32, s);
-  f.kind = 2;
+  coarsest_assemble(f.f, Lc.g, f.S64c, c->C.dof_index, s);
+  coarsest_regularise(f.f, c->dtmp, s);
+  coarsest_factor(f.f, s);
+  const int st1 = coarsest_status(f.f, s);
+  if (st1 < 0) throw std::runtime_error("coarsest-level Cholesky: a grid barrier wait timed out");
+  if (st1 > 0) throw std::runtime_error("coarsest-level Cholesky failed even after eps*I regularisation");
+  f.f.kind = 2;
 }
 
 void coarse_wait_background(topo_ctx* c) {
@@ -564,6 +531,8 @@ void do_setup(topo_ctx* c, const double* E, cudaStream_t s) {
   double st4[4];
   TOPO_CUDA_CHECK(cudaMemcpyAsync(st4, c->dtmp + 8, sizeof(st4), cudaMemcpyDeviceToHost, s));
   TOPO_CUDA_CHECK(cudaStreamSynchronize(s));
+  if (!std::isfinite(st4[0]) || !std::isfinite(st4[1]) || !std::isfinite(st4[2]))
+    throw std::invalid_argument("topo_gmg_setup: the moduli contain NaN or Inf");
   const double Emax = st4[2];
   const bool re = std::isnan(c->lam_Emax) || std::fabs(Emax - c->lam_Emax) / std::max(std::fabs(c->lam_Emax), 1e-12) > 0.10;
   if (re) {
@@ -580,7 +549,7 @@ void do_setup(topo_ctx* c, const double* E, cudaStream_t s) {
     stencil_dinv(Lv.g, Lv.S64, Lv.mask, dinv64, c->vec64 ? nullptr : (float*)Lv.dinv, s);
     if (re || std::isnan(Lv.lam)) Lv.lam = lambda_coarse(c, l, dinv64, s);
     if (Lv.prec == Prec::F32 || Lv.prec == Prec::BF16)
-      stencil_convert(243LL * Lv.g.nnodes, Lv.S64, Lv.S32, Lv.prec == Prec::BF16 ? Lv.S16 : nullptr, s);
+      stencil_convert(Lv.g.nnodes, Lv.S64, Lv.S32, Lv.prec == Prec::BF16 ? Lv.S16 : nullptr, s);
   }
   // coarsest: dense FP64 Cholesky + W = L^-1, one graph per factor slot, with
   // the reference's eps*I retry (multigrid_v4.py:778-811)
@@ -607,8 +576,7 @@ void do_setup(topo_ctx* c, const double* E, cudaStream_t s) {
         slot_finish(c, c->C.nxt, s);
         std::swap(c->C.cur, c->C.nxt);
       }
-      if (!c->C.nxt.A) alloc_slot(c, c->C.nxt);
-      slot_graph(c, c->C.nxt, s);
+      if (!c->C.nxt.S64c) alloc_slot(c, c->C.nxt);
       TOPO_CUDA_CHECK(cudaMemcpyAsync(c->C.nxt.S64c, Lc.S64, sb, cudaMemcpyDeviceToDevice, s));
       TOPO_CUDA_CHECK(cudaEventRecord(c->C.ev_copy, s));
       TOPO_CUDA_CHECK(cudaStreamWaitEvent(c->C.bg_stream, c->C.ev_copy, 0));
@@ -645,8 +613,8 @@ std::vector<double> pcg_graph_key(const topo_ctx* c) {
   std::vector<double> k = {(double)c->cheb_form, c->lam_safety, c->cheb_lower, (double)c->use_tc,
                            (double)c->cycle_gamma,
                            (double)c->fine_degree, (double)c->coarse_degree,
-                           (double)reinterpret_cast<uintptr_t>(c->C.cur.work), (double)reinterpret_cast<uintptr_t>(c->C.cur.X32),
-                           (double)reinterpret_cast<uintptr_t>(c->C.y), (double)c->C.n, (double)c->C.ldc};
+                           (double)reinterpret_cast<uintptr_t>(c->C.cur.f.DI), (double)reinterpret_cast<uintptr_t>(c->C.cur.f.M),
+                           (double)reinterpret_cast<uintptr_t>(c->C.y), (double)c->C.n, (double)c->C.cur.f.plan.nb};
   for (const Level& Lv : c->L) {
     k.push_back(std::isnan(Lv.lam) ? -1.0 : Lv.lam);  // NaN (no estimate) would never compare equal
     k.push_back((double)Lv.degree);
@@ -690,8 +658,10 @@ int do_pcg(topo_ctx* c, const double* b, double* x, double tol, int maxiter, int
   vmask(true, n, c->kx64, L0.mask, s);
   vmask(true, n, c->kb64, L0.mask, s);
   const double bb = dot_host(true, n, c->kb64, c->kb64, c->red, c->dtmp, s);
+  if (!std::isfinite(bb)) throw std::invalid_argument("topo_pcg: the right-hand side contains NaN or Inf");
   const double tol2 = tol * tol * bb;
   double rr = true_residual(c, s);
+  if (!std::isfinite(rr)) throw std::invalid_argument("topo_pcg: the initial guess contains NaN or Inf");
   int iters = 0;
   bool converged = rr <= tol2;  // up-front check (solver_v2.py:594-596)
   // one PCG iteration recorded as a CUDA graph on the context stream, reused
@@ -759,10 +729,12 @@ int do_pcg(topo_ctx* c, const double* b, double* x, double tol, int maxiter, int
     ++refreshes;
   }
   rr = true_residual(c, s);
+  if (c->use_tc && xs_error_flag(s)) throw std::runtime_error("tensor-core K.u: an mbarrier wait timed out");
+  if (!std::isfinite(rr)) throw std::runtime_error("topo_pcg: the iteration produced NaN or Inf");
   TOPO_CUDA_CHECK(cudaMemcpyAsync(x, c->kx64, vb, cudaMemcpyDeviceToDevice, s));
   if (out_iters) *out_iters = iters;
   if (out_relres) *out_relres = bb > 0 ? std::sqrt(rr / bb) : 0.0;
-  if (c->use_tc && tc_error_flag(s)) throw std::runtime_error("tensor-core K.u: an mbarrier wait timed out");
+  if (c->use_tc && xs_error_flag(s)) throw std::runtime_error("tensor-core K.u: an mbarrier wait timed out");
   return converged ? 0 : 1;
 }
 
@@ -1073,7 +1045,7 @@ static void register_ke(topo_ctx* c, const double* KE) {
     std::vector<double> Q(8 * 576);
     host_galerkin_q(KE, Q.data());
     set_galerkin_q(Q.data());
-    tc_prepare(KE);
+    xs_prepare(KE);
     d.ke.assign(KE, KE + 576);
   }
   d.live += 1;
@@ -1145,14 +1117,15 @@ int topo_ctx_create(int nelx, int nely, int nelz, int n_levels, int mode, int fi
       if (l >= 1) {
         Lv.S64 = c->alloc<double>(243LL * Lv.g.nnodes);
         if (l < n_levels - 1) {
-          if (Lv.prec != Prec::F64) Lv.S32 = c->alloc<float>(243LL * Lv.g.nnodes);
-          if (Lv.prec == Prec::BF16) Lv.S16 = c->alloc<__nv_bfloat16>(243LL * Lv.g.nnodes);
+          if (Lv.prec != Prec::F64) Lv.S32 = c->alloc<float>(27LL * 12 * Lv.g.nnodes);
+          if (Lv.prec == Prec::BF16) Lv.S16 = c->alloc<__nv_bfloat16>(27LL * 12 * Lv.g.nnodes);
         }
       }
     }
     const Grid& g0 = c->L[0].g;
     c->E64 = c->alloc<double>(g0.nelem);
     c->E32 = c->alloc<float>(g0.nelem);
+    c->nmask0 = c->alloc<uint8_t>(g0.nnodes + 16);
     c->diag0 = c->alloc<double>(g0.ndof);
     c->kr = c->valloc(g0.ndof);
     c->kz = c->valloc(g0.ndof);
@@ -1199,8 +1172,6 @@ int topo_ctx_destroy(topo_ctx* c) {
   if (c->blk_Gh) cudaFreeHost(c->blk_Gh);
   if (c->pcg_exec) cudaGraphExecDestroy(c->pcg_exec);
   if (c->C.bg_pending && c->C.bg_done) cudaEventSynchronize(c->C.bg_done);
-  for (FactorSlot* f : {&c->C.cur, &c->C.nxt})
-    if (f->graph) cudaGraphExecDestroy(f->graph);
   if (c->C.ev_copy) cudaEventDestroy(c->C.ev_copy);
   if (c->C.bg_done) cudaEventDestroy(c->C.bg_done);
   if (c->C.bg_stream) cudaStreamDestroy(c->C.bg_stream);
@@ -1245,6 +1216,8 @@ int topo_set_problem(topo_ctx* c, const uint8_t* free_mask, const double* F, voi
     TOPO_CUDA_CHECK(cudaMemcpyAsync(L0.mask, free_mask, L0.g.ndof, cudaMemcpyDeviceToDevice, s));
     TOPO_CUDA_CHECK(cudaMemcpyAsync(c->Fvec, F, sizeof(double) * L0.g.ndof, cudaMemcpyDeviceToDevice, s));
     for (int l = 1; l < c->n_levels; ++l) inject_mask(c->L[l - 1].g, c->L[l].g, c->L[l - 1].mask, c->L[l].mask, s);
+    k_node_mask<<<gblocks(L0.g.nnodes), 256, 0, s>>>(L0.g.nnodes, L0.mask, c->nmask0);
+    TOPO_LAUNCH_CHECK();
     // coarsest compact numbering and band
     if (c->n_levels > 1) {
       Level& Lc = c->L[c->n_levels - 1];
@@ -1278,17 +1251,24 @@ int topo_set_problem(topo_ctx* c, const uint8_t* free_mask, const double* F, voi
       }
       coarse_wait_background(c);
       c->C.have = false;
-      if (c->C.n != n || c->C.cur.A == nullptr) {
+      CoarsestPlan plan = coarsest_plan(Lc.g, fl);
+      if (!coarsest_supported(plan))
+        throw std::runtime_error("coarsest level has an x-plane with " + std::to_string(plan.mmax) +
+                                 " free DoFs, above the 512 the direct solve supports; use more levels");
+      if (c->C.n != n || c->C.band != band || c->C.cur.S64c == nullptr || plan.boff != c->C.plan.boff) {
         c->C.n = n;
+        c->C.band = band;
+        c->C.plan = plan;
         c->C.dof_index = c->alloc<int>(Lc.g.ndof);
         c->C.free_list = c->alloc<int>(std::max(n, 1));
-        c->C.ldc = ((n + 31) / 32) * 32;
-        c->C.y = c->alloc<double>(2 * (size_t)std::max(n, 1));  // y, then the compact rhs
+        c->C.y = c->alloc<double>(2 * (size_t)std::max(n, 1));
+        c->C.cur = FactorSlot();
         alloc_slot(c, c->C.cur);
-        if (c->C.nxt.A) alloc_slot(c, c->C.nxt);
-        dense_apply_prepare(n);
+        if (c->C.nxt.S64c) {
+          c->C.nxt = FactorSlot();
+          alloc_slot(c, c->C.nxt);
+        }
       }
-      c->C.band = band;
       TOPO_CUDA_CHECK(cudaMemcpyAsync(c->C.dof_index, idx.data(), sizeof(int) * idx.size(), cudaMemcpyHostToDevice, s));
       TOPO_CUDA_CHECK(cudaMemcpyAsync(c->C.free_list, fl.data(), sizeof(int) * std::max<size_t>(fl.size(), 1),
                                       cudaMemcpyHostToDevice, s));
@@ -1323,14 +1303,78 @@ int topo_matvec(topo_ctx* c, int dtype, const void* u, void* y, const void* E, v
     if (dtype == TOPO_F64) level0_apply(Prec::F64, L0.g, u, E, L0.mask, y, Epi::Store, ea, c->cs);
     else if (dtype == TOPO_F32) level0_apply(Prec::F32, L0.g, u, E, L0.mask, y, Epi::Store, ea, c->cs);
     else if (dtype == TOPO_BF16) {
-      if (c->use_tc) level0_apply_tc(true, L0.g, u, E, L0.mask, y, Epi::Store, ea, c->cs);
-      else level0_apply_bf16_input(L0.g, u, E, L0.mask, y, c->cs);
+      if (c->use_tc && level0_xs_supported(L0.g)) {
+        level0_apply_xs(true, L0.g, u, E, c->nmask0, y, Epi::Store, ea, c->cs);
+        if (xs_error_flag(c->cs)) throw std::runtime_error("tensor-core K.u: an mbarrier wait timed out");
+      } else {
+        level0_apply_bf16_input(L0.g, u, E, L0.mask, y, c->cs);
+      }
     }
     else throw std::invalid_argument("topo_matvec: bad dtype");
     return 0;
   } catch (const std::exception& e) {
     return fail(c, e);
   }
+}
+
+int topo_level0_apply(topo_ctx* c, int u_dtype, int epi, const void* u, const void* E, void* y, const void* b, void* r,
+                      void* x, void* d_out, const void* dinv, double s, double c1, double c2, double ax,
+                      void* stream) {
+  try {
+    if (!c || !u || !E) throw std::invalid_argument("topo_level0_apply: null pointer");
+    if (!c->problem_set) throw std::runtime_error("topo_level0_apply: call topo_set_problem first");
+    Epi ep;
+    switch (epi) {
+      case TOPO_EPI_STORE: ep = Epi::Store; if (!y) throw std::invalid_argument("topo_level0_apply: y is null"); break;
+      case TOPO_EPI_RESIDUAL:
+        ep = Epi::Residual;
+        if (!y || !b) throw std::invalid_argument("topo_level0_apply: residual needs y and b");
+        break;
+      case TOPO_EPI_RUPD: ep = Epi::RUpd; if (!r) throw std::invalid_argument("topo_level0_apply: r is null"); break;
+      case TOPO_EPI_CHEB:
+        ep = Epi::ChebR;
+        if (!r || !x || !d_out || !dinv) throw std::invalid_argument("topo_level0_apply: Chebyshev step needs r, x, d_out, dinv");
+        if (d_out == u) throw std::invalid_argument("topo_level0_apply: d_out must differ from u");
+        break;
+      default: throw std::invalid_argument("topo_level0_apply: bad epilogue");
+    }
+    StreamGuard sg(c, stream);
+    Level& L0 = c->L[0];
+    EpiArgs ea{};
+    ea.b = b;
+    ea.r = r;
+    ea.x = x;
+    ea.d_out = d_out;
+    ea.dinv = dinv;
+    ea.s = s;
+    ea.c1 = c1;
+    ea.c2 = c2;
+    ea.ax = ax;
+    if (u_dtype == TOPO_F64) level0_apply(Prec::F64, L0.g, u, E, L0.mask, y, ep, ea, c->cs);
+    else if (u_dtype == TOPO_F32) level0_apply(Prec::F32, L0.g, u, E, L0.mask, y, ep, ea, c->cs);
+    else if (u_dtype == TOPO_BF16 || u_dtype == TOPO_BF16_F32IN) {
+      const bool u16 = u_dtype == TOPO_BF16;
+      if (c->use_tc && level0_xs_supported(L0.g)) {
+        level0_apply_xs(u16, L0.g, u, E, c->nmask0, y, ep, ea, c->cs);
+        if (xs_error_flag(c->cs)) throw std::runtime_error("tensor-core K.u: an mbarrier wait timed out");
+      } else if (!u16) {
+        level0_apply(Prec::BF16, L0.g, u, E, L0.mask, y, ep, ea, c->cs);
+      } else {
+        if (ep != Epi::Store) throw std::runtime_error("topo_level0_apply: BF16-stored u on CUDA cores supports Store only");
+        level0_apply_bf16_input(L0.g, u, E, L0.mask, y, c->cs);
+      }
+    } else {
+      throw std::invalid_argument("topo_level0_apply: bad dtype");
+    }
+    return 0;
+  } catch (const std::exception& e) {
+    return fail(c, e);
+  }
+}
+
+int topo_debug_tc_wait(int skip_first_arrival, int poll_limit) {
+  xs_debug(skip_first_arrival, poll_limit);
+  return 0;
 }
 
 int topo_diag(topo_ctx* c, const double* E, double* diag, void* stream) {
@@ -1363,7 +1407,7 @@ int topo_gmg_apply(topo_ctx* c, const void* r, void* z, void* stream) {
     if (!c->setup_done) throw std::runtime_error("topo_gmg_apply: call topo_gmg_setup first");
     StreamGuard sg(c, stream);
     vcycle_apply(c, r, z, nullptr, c->cs);
-    if (c->use_tc && tc_error_flag(c->cs)) throw std::runtime_error("tensor-core K.u: an mbarrier wait timed out");
+    if (c->use_tc && xs_error_flag(c->cs)) throw std::runtime_error("tensor-core K.u: an mbarrier wait timed out");
     return 0;
   } catch (const std::exception& e) {
     return fail(c, e);
@@ -1576,7 +1620,7 @@ int topo_gmg_info(topo_ctx* c, long long* n_free, double* lambda_max, int* coars
       }
       if (lambda_max) lambda_max[l] = c->L[l].lam;
     }
-    if (coarse_kind) *coarse_kind = c->C.cur.kind;
+    if (coarse_kind) *coarse_kind = c->C.cur.f.kind;
     return 0;
   } catch (const std::exception& e) {
     return fail(c, e);

@@ -9,6 +9,7 @@
 #include <algorithm>
 #include <stdexcept>
 #include <string>
+#include <vector>
 
 namespace topo {
 
@@ -209,11 +210,15 @@ __device__ __forceinline__ void epilogue_store(const EpiDev<T>& e, long long i, 
 void level0_apply(Prec p, const Grid& g, const void* u, const void* E, const uint8_t* mask, void* y,
                   Epi epi, const EpiArgs& ea, cudaStream_t s);
 void level0_diag(const Grid& g, const double* E, const uint8_t* mask, double* diag, cudaStream_t s);
-// tensor-core BF16-input operator (kmatvec_tc.cu)
-void tc_prepare(const double* KE_host);
-void level0_apply_tc(bool u_bf16, const Grid& g, const void* u, const void* E, const uint8_t* mask, void* y, Epi epi,
+// tensor-core BF16-input operator streaming along x (kmatvec_xs.cu); the
+// KE tile and the error flag are per device
+void xs_prepare(const double* KE_host);
+bool level0_xs_supported(const Grid& g);
+// nmask: per-node free bits (bit c = DoF 3n+c free)
+void level0_apply_xs(bool u_bf16, const Grid& g, const void* u, const void* E, const uint8_t* nmask, void* y, Epi epi,
                      const EpiArgs& ea, cudaStream_t s);
-int tc_error_flag(cudaStream_t s);
+int xs_error_flag(cudaStream_t s);
+void xs_debug(int skip_first_arrival, int poll_limit);
 void modulus(long long n, const double* rho, double penal, double E0, double Emin, double* E,
              float* E32, cudaStream_t s);
 // dc_e = -penal (E0-Emin) rho_e^(penal-1) v_e^T KE u_e (v = u when null)
@@ -229,29 +234,50 @@ void stencil_apply(Prec p, bool vec64, const Grid& g, const void* S, const void*
                    void* y, Epi epi, const EpiArgs& ea, cudaStream_t s);
 void stencil_dinv(const Grid& g, const double* S, const uint8_t* mask, double* dinv64, float* dinv32,
                   cudaStream_t s);
-void stencil_convert(long long n, const double* S, float* S32, __nv_bfloat16* S16, cudaStream_t s);
+// FP64 coefficient-major stencil -> packed FP32 / BF16 apply copies (27*12 values per node)
+void stencil_convert(long long nnodes, const double* S, float* S32, __nv_bfloat16* S16, cudaStream_t s);
 void inject_mask(const Grid& fine, const Grid& coarse, const uint8_t* mf, uint8_t* mc, cudaStream_t s);
 void restrict_vec(bool vec64, const Grid& fine, const Grid& coarse, const void* rf, const uint8_t* mc,
                   void* rc, const KrylovState* st, cudaStream_t s);
 // x_f += e = mask_f * P e_c ; e is also written to e_out when not null
 void prolong_add(bool vec64, const Grid& fine, const Grid& coarse, const void* ec, const uint8_t* mf,
                  void* xf, void* e_out, const KrylovState* st, cudaStream_t s);
-void dense_assemble(const Grid& g, const double* S, const int* dof_index, int n, double* A,
+// coarsest level (coarsest.cu): band Cholesky of the free-DoF operator and
+// block sweeps over its x-plane blocks. Compact DoF i -> full DoF free[i].
+struct CoarsestPlan {
+  int n = 0, nb = 0, mmax = 0;
+  std::vector<int> boff, link;              // block b = compact rows [boff[b], boff[b+1]); link[b]: couples to b-1
+  std::vector<long long> dioff, moff, noff; // offsets of Di_b, M_b (and L_{b,b-1}), N_b
+  long long di_size = 0, m_size = 0, n_size = 0;
+};
+struct CoarsestFactor {
+  CoarsestPlan plan;
+  int band = 0;
+  long long ldb = 0;
+  bool f64 = true;                          // apply matrices and vectors in FP64 (else FP32)
+  double *A = nullptr, *L = nullptr;        // band storage (n x (band+1)): operator, factor
+  double *DI64 = nullptr, *LS64 = nullptr;  // Di_b and L_{b,b-1} in FP64
+  void *DI = nullptr, *M = nullptr, *N = nullptr;  // apply matrices
+  int* flag = nullptr;                      // [0] non-positive pivot, [1] barrier timeout
+  int* err = nullptr;
+  unsigned* bar = nullptr;
+  int *d_boff = nullptr, *d_link = nullptr;
+  long long *d_dioff = nullptr, *d_moff = nullptr, *d_noff = nullptr;
+  void* d_jobs = nullptr;
+  int njobs = 0, chol_grid = 1;
+  const int* d_free = nullptr;
+  int kind = 0;                             // 0 none, 1 Cholesky, 2 Cholesky of K + eps I
+};
+CoarsestPlan coarsest_plan(const Grid& g, const std::vector<int>& free_list);
+bool coarsest_supported(const CoarsestPlan& p);
+void coarsest_alloc(CoarsestFactor& f, const CoarsestPlan& p, int band, bool f64, void* (*alloc_bytes)(void*, size_t),
+                    void* ctx);
+void coarsest_assemble(CoarsestFactor& f, const Grid& g, const double* S, const int* dof_index, cudaStream_t s);
+void coarsest_regularise(CoarsestFactor& f, double* dtmp, cudaStream_t s);
+void coarsest_factor(CoarsestFactor& f, cudaStream_t s);
+int coarsest_status(CoarsestFactor& f, cudaStream_t s);
+void coarsest_apply(const CoarsestFactor& f, bool vec64, const void* rhs, double* work, void* x, const KrylovState* st,
                     cudaStream_t s);
-// Banded Cholesky in place (off-diagonal band of L in A's lower part, the
-// factored diagonal blocks in Dt); returns 0 on success, 1 if a pivot was not
-// positive/finite (host sync inside).
-int dense_cholesky(int n, int band, double* A, double* Dt, int* flag, cudaStream_t s);
-// the same launches without the flag read-back (capturable; flag checked later)
-void dense_cholesky_launch(int n, int band, double* A, double* Dt, int* flag, cudaStream_t s);
-// W = L^-1 into W64 (FP64, lower) and into the apply matrices C64/C32 (W
-// lower, W^T upper); Di receives the inverses of the diagonal blocks.
-void dense_inverse_factor(int n, int band, const double* A, const double* Dt, double* Di, double* W64,
-                          long long ldc, double* C64, float* C32, cudaStream_t s);
-void dense_apply_prepare(int n);
-// x = scatter(W^T W gather(rhs)); y is n FP64 scratch
-void dense_apply(bool vec64, int n, long long ldc, const double* C64, const float* C32, const int* free_list,
-                 const void* rhs, double* y, void* x, const KrylovState* st, cudaStream_t s);
 
 // block PCG kernels (blockops.cu): FP64 column blocks as pointer lists
 void set_ke_block(const double* KE_host);

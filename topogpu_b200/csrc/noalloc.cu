@@ -20,6 +20,7 @@
 #include "../../include/topo_b200.h"
 
 #include <cmath>
+#include <mutex>
 #include <string>
 
 namespace topo {
@@ -105,14 +106,18 @@ __global__ void k_final(long long n, const double* __restrict__ rho, const doubl
 
 // Device address of g_oc_scratch per device, looked up once per device with
 // that device current (the symbol's host-side name is not a device address).
+// The table is guarded by a mutex: two host threads making their first call
+// on the same device at once would otherwise race on it.
 constexpr int kMaxDevices = 64;
 static double* g_scratch_ptr[kMaxDevices] = {};
+static std::mutex g_scratch_mu;
 
 static double* scratch_for_current_device() {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) throw std::runtime_error(std::string("cudaGetDevice: ") + cudaGetErrorString(e));
   if (dev < 0 || dev >= kMaxDevices) throw std::runtime_error("topo_oc_noalloc: device ordinal out of range");
+  std::lock_guard<std::mutex> lk(g_scratch_mu);
   if (g_scratch_ptr[dev] == nullptr) {
     double* p = nullptr;
     e = cudaGetSymbolAddress((void**)&p, g_oc_scratch);
@@ -134,6 +139,7 @@ extern "C" int topo_oc_noalloc(const double* rho, const double* dc, long long n,
       throw std::invalid_argument("topo_oc_noalloc: n = " + std::to_string(n) + " is outside [1, " +
                                   std::to_string(kMaxElems) + "], the size its static scratch serves");
     if (!rho || !dc || !out) throw std::invalid_argument("topo_oc_noalloc: null pointer");
+    if (out == rho || out == dc) throw std::invalid_argument("topo_oc_noalloc: out must not alias rho or dc");
     cudaStream_t s = (cudaStream_t)stream;
     double* scr = scratch_for_current_device();
     k_init<<<1, 1, 0, s>>>(scr);

@@ -33,12 +33,17 @@ class MatrixFreeOperator:
 
 
 class GMGPreconditioner:
-    """Galerkin GMG hierarchy with Chebyshev-Jacobi smoothing."""
+    """Galerkin GMG hierarchy with Chebyshev-Jacobi smoothing.
+
+    smoother="reference" applies the reference's Chebyshev recurrence
+    (multigrid_v4.py:861-889) and reproduces its V-cycle; the default
+    "chebyshev" is the first-kind Chebyshev iteration with a 1.25 safety
+    factor on lambda_max (the product default)."""
 
     def __init__(self, nel, free_mask, F=None, n_levels=4, precision="fp64", fine_degree=2, coarse_degree=2,
-                 cheb_lower=1.0 / 30.0, device=None):
+                 cheb_lower=1.0 / 30.0, device=None, smoother="chebyshev"):
         self.ctx = TopoContext(nel, n_levels=n_levels, mode=precision, fine_degree=fine_degree,
-                               coarse_degree=coarse_degree, cheb_lower=cheb_lower)
+                               coarse_degree=coarse_degree, cheb_lower=cheb_lower, smoother=smoother)
         dev = device or torch.device("cuda", torch.cuda.current_device())
         self.free_mask = torch.as_tensor(np.asarray(free_mask, dtype=np.uint8), device=dev).contiguous()
         F = torch.zeros(self.ctx.ndof, dtype=torch.float64, device=dev) if F is None else \
