@@ -18,7 +18,7 @@ from pathlib import Path
 PKG = Path(__file__).resolve().parent
 CSRC = PKG / "csrc"
 OUT = PKG / "libtopo_b200.so"
-SOURCES = ["level0.cu", "kmatvec_xs.cu", "coarse.cu", "coarsest.cu", "vec.cu", "design.cu", "blockops.cu", "ctx.cu", "noalloc.cu"]
+SOURCES = ["level0.cu", "kmatvec_xs.cu", "kmatvec_cc.cu", "coarse.cu", "coarsest.cu", "vec.cu", "design.cu", "blockops.cu", "ctx.cu", "noalloc.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-diag-suppress", "177"]
 

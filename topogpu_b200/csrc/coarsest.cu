@@ -479,7 +479,7 @@ __global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(AT)
         double acc = 0.0;
         for (int j = lane; j < mp; j += 32) acc += (double)Mb[(long long)i * mp + j] * vb[j];
         acc = warp_sum(acc);
-        if (lane == 0) y[o + i] -= acc;
+        if (lane == 0) y[o + i] = __ldcg(y + o + i) - acc;
       }
       __syncthreads();
     }
@@ -507,7 +507,7 @@ __global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(AT)
         double acc = 0.0;
         for (int j = lane; j < mn; j += 32) acc += (double)Nb[(long long)i * mn + j] * vb[j];
         acc = warp_sum(acc);
-        if (lane == 0) z[o + i] -= acc;
+        if (lane == 0) z[o + i] = __ldcg(z + o + i) - acc;
       }
       __syncthreads();
     }

@@ -218,6 +218,11 @@ bool level0_xs_supported(const Grid& g);
 void level0_apply_xs(bool u_bf16, const Grid& g, const void* u, const void* E, const uint8_t* nmask, void* y, Epi epi,
                      const EpiArgs& ea, cudaStream_t s);
 int xs_error_flag(cudaStream_t s);
+int* wait_error_flag();
+// FP32 / FP64 level-0 K.u on the CUDA cores streaming along x (kmatvec_cc.cu)
+bool level0_cc_supported(const Grid& g, bool f64);
+void level0_apply_cc(bool f64, const Grid& g, const void* u, const void* E, const uint8_t* mask, void* y, Epi epi,
+                     const EpiArgs& ea, int* err, cudaStream_t s);
 void xs_debug(int skip_first_arrival, int poll_limit);
 void modulus(long long n, const double* rho, double penal, double E0, double Emin, double* E,
              float* E32, cudaStream_t s);

@@ -905,6 +905,14 @@ int xs_error_flag(cudaStream_t s) {
   return h;
 }
 
+// The device's wait-timeout flag shared by the streaming kernels (allocated
+// when the device's KE tile is prepared, so never during a stream capture).
+int* wait_error_flag() {
+  XsDevice& d = xs_device();
+  if (!d.err) throw std::runtime_error("streaming K.u: device not prepared");
+  return d.err;
+}
+
 void xs_debug(int skip_first_arrival, int poll_limit) {
   std::lock_guard<std::mutex> lk(g_xs_mu);
   g_xs_skip = skip_first_arrival ? 1 : 0;

@@ -246,9 +246,19 @@ static void launch_level0(const Grid& g, const void* u, const void* E, const uin
 
 void level0_apply(Prec p, const Grid& g, const void* u, const void* E, const uint8_t* mask, void* y, Epi epi,
                   const EpiArgs& ea, cudaStream_t s) {
+  // FP64 / FP32: the x-streaming kernel (kmatvec_cc.cu) when its planes fit
+  // in shared memory; the brick kernel below otherwise and for the BF16
+  // emulation on CUDA cores.
+  const bool al = ((uintptr_t)u & 15) == 0 && ((uintptr_t)E & 15) == 0;
   switch (p) {
-    case Prec::F64: launch_level0<double, double, false>(g, u, E, mask, y, epi, ea, s); break;
-    case Prec::F32: launch_level0<float, float, false>(g, u, E, mask, y, epi, ea, s); break;
+    case Prec::F64:
+      if (al && level0_cc_supported(g, true)) level0_apply_cc(true, g, u, E, mask, y, epi, ea, wait_error_flag(), s);
+      else launch_level0<double, double, false>(g, u, E, mask, y, epi, ea, s);
+      break;
+    case Prec::F32:
+      if (al && level0_cc_supported(g, false)) level0_apply_cc(false, g, u, E, mask, y, epi, ea, wait_error_flag(), s);
+      else launch_level0<float, float, false>(g, u, E, mask, y, epi, ea, s);
+      break;
     case Prec::BF16: launch_level0<float, float, true>(g, u, E, mask, y, epi, ea, s); break;
   }
 }
