@@ -216,3 +216,85 @@ def test_two_level_balanced_schwarz_flattens_the_iteration_count(precond):
     print(f"PCG iterations to 1e-10, {precond} pieces: two-level {two}, one-level at 4 slabs {one}")
     assert two[4] <= 1.2 * two[2]
     assert two[4] < 0.75 * one
+
+
+def _simp_rank(rank, world, port, nel, rmin, out):
+    import torch
+    import torch.distributed as dist
+
+    sys.path.insert(0, str(ROOT))
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        from oracle import fem
+        from topogpu_b200.slab import Slab, SlabCoarse, SlabFilter, SlabPCG, all_dots, coarse_prolongation, \
+            element_halo, slab_oc_filtered
+
+        bc = fem.cantilever_bc(nel)
+        bc.free_mask = lambda: _bc_free_mask(bc)
+        slab = Slab.of(nel, rank, world, overlap=1)
+        per = nel[1] * nel[2]
+        ea, eb = slab.element_range(slab.e0, slab.e1)
+        rho_g = np.random.default_rng(3).uniform(0.2, 0.9, int(np.prod(nel)))
+        rho = torch.as_tensor(rho_g[ea:eb].copy())
+        filt = SlabFilter(slab, rmin, dist)
+        rho_f = filt.apply(rho)
+        E_own = 1e-9 + (1 - 1e-9) * rho_f ** 3
+        # the moduli the Schwarz pieces need (layers x_lo .. x_hi) from the halo
+        hh = max(slab.e0 - slab.x_lo, slab.x_hi - slab.e1)
+        E_ext = element_halo(E_own, slab, hh, dist).numpy()
+        E_glob = np.zeros(int(np.prod(nel)))
+        lo = max(slab.e0 - hh, 0)
+        E_glob[lo * per:lo * per + len(E_ext)] = E_ext
+        ops = OracleSlabOps(slab, bc, E_glob, "exact")
+        P0 = coarse_prolongation(nel, _bc_free_mask(bc), 1)
+        a, b = slab.dof_range()
+        P = torch.as_tensor(P0[a:b].toarray())
+        coarse = SlabCoarse(slab, P, SlabCoarse.galerkin(slab, P, ops.matvec, dist), dist)
+        pcg = SlabPCG(slab, ops, dist, coarse=coarse, balanced=True)
+        F = torch.as_tensor((bc.F * _bc_free_mask(bc))[a:b].copy())
+        u, it, rr, ok = pcg.solve(F, tol=1e-13, maxiter=400)
+        (c,) = all_dots([(F, u)], pcg.w, dist, world)
+        dc = torch.as_tensor(fem.sensitivity(u.numpy(), rho_f.numpy(), slab.local_nel))
+        dcd = filt.apply_transpose(dc)
+        colsum = filt.apply_transpose(torch.ones_like(rho))
+        rho_new, k = slab_oc_filtered(rho, dcd, colsum, colsum, 0.3, 0.2, slab, dist)
+        out[rank] = {"rho_new": rho_new.numpy(), "rho_f": rho_f.numpy(), "c": c, "evals": k, "ok": ok,
+                     "ea": ea, "eb": eb}
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world,rmin", [(2, 2.0), (3, 1.5), (4, 2.3)])
+def test_slab_simp_step_matches_single_process(world, rmin):
+    """One filtered SIMP iteration on slabs (distributed filter with a halo
+    of floor(rmin) element layers, two-level slab PCG, local sensitivities,
+    H^T chain, filtered OC with the volume all-reduced per bisection step)
+    against the undivided oracle step with a direct solve: filtered density
+    to round-off, compliance and the new density to 1e-8, same number of OC
+    evaluations."""
+    from oracle import design, fem
+
+    nel = (16, 4, 4)
+    port = _free_port()
+    with mp.Manager() as m:
+        out = m.dict()
+        mp.spawn(_simp_rank, args=(world, port, nel, rmin, out), nprocs=world, join=True)
+        res = dict(out)
+    bc = fem.cantilever_bc(nel)
+    rho = np.random.default_rng(3).uniform(0.2, 0.9, int(np.prod(nel)))
+    H = design.filter_matrix(nel, rmin)
+    rf = H @ rho
+    E = fem.simp_modulus(rf)
+    U = fem.direct_solve(E, nel, bc)
+    c_ref = float(bc.F @ U)
+    dc = fem.sensitivity(U, rf, nel)
+    dv = H.T @ np.ones(len(rho))
+    ref, k_ref = design.oc_update_filtered(rho, H.T @ dc, dv, 0.3, 0.2, H)
+    for r in res.values():
+        assert r["ok"]
+        np.testing.assert_allclose(r["rho_f"], rf[r["ea"]:r["eb"]], rtol=1e-13, atol=1e-15)
+        assert abs(r["c"] - c_ref) / c_ref < 1e-8
+        assert r["evals"] == k_ref
+        np.testing.assert_allclose(r["rho_new"], ref[r["ea"]:r["eb"]], rtol=1e-8, atol=1e-10)

@@ -428,6 +428,116 @@ class SlabPCG:
         return x, maxiter, np.sqrt(rr) / bn, False
 
 
+# ----------------------------------------------------- design update on slabs
+def element_halo(x: torch.Tensor, slab: Slab, h: int, dist) -> torch.Tensor:
+    """Element field of the rank's layers [e0, e1) -> layers
+    [max(e0-h, 0), min(e1+h, nelx)) with the neighbours' layers (h must not
+    exceed any slab's layer count)."""
+    if slab.world == 1 or h == 0:
+        return x
+    per = slab.nel[1] * slab.nel[2]
+    hl = min(h, slab.e0) * per
+    hr = min(h, slab.nel[0] - slab.e1) * per
+    got_l, got_r = _exchange(slab, dist, x[:h * per], x[-h * per:], hl, hr, x)
+    parts = ([got_l] if got_l is not None else []) + [x] + ([got_r] if got_r is not None else [])
+    return torch.cat(parts)
+
+
+class SlabFilter:
+    """The linear-hat density filter of run_simp (neighbours at centre
+    distance <= rmin - 1e-10, weight rmin - d, the element itself weight rmin,
+    rows normalised; src/gpu_fem/pub_simp_solver.py:215-243) on one rank's
+    element layers. H x needs floor(rmin) halo layers of x from each
+    neighbour; H^T x needs the same halo of x / Hs. The row sums Hs depend on
+    the global position only, so every rank computes them itself."""
+
+    def __init__(self, slab: Slab, rmin: float, dist, device="cpu"):
+        import math
+
+        self.slab, self.dist, self.rmin = slab, dist, float(rmin)
+        self.h = R = int(math.floor(rmin))
+        if slab.world > 1 and R > min(b - a for a, b in partition(slab.nel[0], slab.world)):
+            raise ValueError("filter radius larger than a slab")
+        self.offsets = []
+        for dx in range(-R, R + 1):
+            for dy in range(-R, R + 1):
+                for dz in range(-R, R + 1):
+                    d = math.sqrt(float(dx * dx + dy * dy + dz * dz))
+                    if dx == dy == dz == 0:
+                        self.offsets.append((0, 0, 0, rmin))
+                    elif d <= rmin - 1e-10:
+                        self.offsets.append((dx, dy, dz, rmin - d))
+        nx, ny, nz = slab.nel
+        ones = torch.ones(nx, ny, nz, dtype=torch.float64, device=device)
+        lo = max(slab.e0 - R, 0)
+        self.Hs = self._stencil(ones[lo:min(slab.e1 + R, nx)], lo)
+
+    def _stencil(self, xe: torch.Tensor, g_lo: int) -> torch.Tensor:
+        """sum over the offsets of w * x[e + offset] for the rank's elements
+        e, neighbours outside the mesh left out; xe holds the global layers
+        g_lo .. (layers, ny, nz), covering every source layer."""
+        R = self.h
+        nx = self.slab.nel[0]
+        pad = torch.nn.functional.pad(xe, (R, R, R, R))  # zero y/z padding (outside the mesh)
+        e0, e1 = self.slab.e0, self.slab.e1
+        out = torch.zeros(e1 - e0, xe.shape[1], xe.shape[2], dtype=xe.dtype, device=xe.device)
+        ny, nz = xe.shape[1], xe.shape[2]
+        for dx, dy, dz, w in self.offsets:
+            a, b = e0 + dx, e1 + dx  # source layers for the owned outputs
+            lo, hi = max(a, 0), min(b, nx)
+            if lo >= hi:
+                continue
+            src = pad[lo - g_lo:hi - g_lo, R + dy:R + dy + ny, R + dz:R + dz + nz]
+            out[lo - a:hi - a] += w * src
+        return out
+
+    def _ext(self, x: torch.Tensor) -> tuple[torch.Tensor, int]:
+        ny, nz = self.slab.nel[1], self.slab.nel[2]
+        xe = element_halo(x, self.slab, self.h, self.dist)
+        return xe.view(-1, ny, nz), max(self.slab.e0 - self.h, 0)
+
+    def apply(self, x: torch.Tensor) -> torch.Tensor:
+        """(H x) on the rank's elements."""
+        xe, g_lo = self._ext(x)
+        return (self._stencil(xe, g_lo) / self.Hs).reshape(-1)
+
+    def apply_transpose(self, x: torch.Tensor) -> torch.Tensor:
+        """(H^T x) on the rank's elements: sum_i w_ij x_i / Hs_i (the weights
+        are symmetric, and the neighbours' x / Hs arrive in the halo)."""
+        xe, g_lo = self._ext((x.view_as(self.Hs) / self.Hs).reshape(-1))
+        return self._stencil(xe, g_lo).reshape(-1)
+
+
+def slab_oc_filtered(rho, dc, dv, colsum, volfrac, move, slab: Slab, dist, rho_min=1e-3):
+    """The filtered-volume OC bisection of run_simp (pub_simp_solver.py:
+    319-340: l1 = 0, l2 = 1e9, at most 100 steps, stop when l2 - l1 < 1e-9,
+    volume measured on H * candidate) on the rank's elements: the volume
+    sum_i (H rn)_i = sum_j rn_j colsum_j (colsum = H^T 1) is all-reduced once
+    per bisection step, so every rank takes the same steps. Returns
+    (candidate, number of evaluations)."""
+    n = float(np.prod(slab.nel))
+    dcs = torch.clamp(dc, max=-1e-12)
+    dvs = torch.clamp(dv, min=1e-12)
+    l1, l2 = 0.0, 1e9
+    rn = rho
+    k = 0
+    for k in range(100):
+        lm = 0.5 * (l1 + l2)
+        rn = rho * torch.sqrt(-dcs / (lm * dvs))
+        rn = torch.minimum(torch.maximum(rn, rho - move), rho + move)
+        rn = torch.clamp(rn, min=rho_min, max=1.0)
+        vol = (rn * colsum).sum().reshape(1)
+        if slab.world > 1:
+            dist.all_reduce(vol)
+        if float(vol) / n > volfrac:
+            l1 = lm
+        else:
+            l2 = lm
+        if l2 - l1 < 1e-9:
+            break
+    return rn, k + 1
+
+
 class CudaSlabOps:
     """``SlabLocalOps`` on the GPU through libtopo_b200: the slab's K u by a
     one-level context on elements [e0, e1), the Schwarz piece by a GMG
