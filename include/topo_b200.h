@@ -131,6 +131,16 @@ int topo_level0_apply(topo_ctx* ctx, int u_dtype, int epi, const void* u, const 
  * returns an error. Applies to later launches in this process. */
 int topo_debug_tc_wait(int skip_first_arrival, int poll_limit);
 
+/* Index range checks (no reference counterpart). In the library built with
+ * -DTOPO_DEBUG_BOUNDS (libtopo_b200_dbg.so: python -m topogpu_b200.build
+ * --debug-bounds) every checked gather/scatter index of the kernels is
+ * tested before the access; an out-of-range index skips the access and
+ * raises a device flag. *tripped receives 1 when a check failed since the
+ * last call (the flags are then cleared), else 0; synchronises the device.
+ * Returns 0 in that build and 1 (checks not compiled, *tripped = 0) in the
+ * normal one. */
+int topo_debug_bounds(int* tripped);
+
 /* diag(K(E)) on all DoFs (zero at fixed DoFs).
  * Replaces MatrixFreeKff.extract_diagonal (src/gpu_fem/solver_v2.py:1229-1252). */
 int topo_diag(topo_ctx* ctx, const double* E, double* diag, void* stream);

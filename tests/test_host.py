@@ -219,3 +219,27 @@ def test_checkpoint_format_matches_reference(tmp_path):
     # a missing half means no checkpoint, as in the reference
     shutil.copy(src + ".npz", tmp_path / "only.npz")
     assert load_checkpoint(str(tmp_path / "only")) is None
+
+
+def test_range_checked_build_compiles_and_exports_every_symbol():
+    """The TOPO_DEBUG_BOUNDS variant (libtopo_b200_dbg.so) builds and exports
+    the same entry points; the normal build reports that it has no checks."""
+    import subprocess
+    import sys
+
+    from topogpu_b200 import _lib, build
+
+    path = build.build(debug_bounds=True)
+    assert path.name == "libtopo_b200_dbg.so"
+    header = (ROOT / "include" / "topo_b200.h").read_text()
+    declared = set(re.findall(r"^\s*(?:int|long long)\s+(topo_\w+)\s*\(", header, flags=re.M))
+    dbg = ctypes.CDLL(str(path))
+    for name in declared:
+        assert hasattr(dbg, name), name
+    lib = _lib.load()
+    t = ctypes.c_int(7)
+    assert lib.topo_debug_bounds(ctypes.byref(t)) == 1 and t.value == 0
+    code = "from topogpu_b200 import _lib; print(_lib.lib_path().name)"
+    out = subprocess.run([sys.executable, "-c", code], cwd=ROOT, env={**__import__("os").environ, "TOPO_B200_LIB": "dbg"},
+                         capture_output=True, text=True, check=True)
+    assert out.stdout.strip() == "libtopo_b200_dbg.so"

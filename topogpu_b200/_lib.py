@@ -9,7 +9,11 @@ from __future__ import annotations
 import ctypes as C
 from pathlib import Path
 
-_LIB_PATH = Path(__file__).resolve().parent / "libtopo_b200.so"
+import os
+
+# TOPO_B200_LIB=dbg loads the range-checked build (python -m topogpu_b200.build --debug-bounds)
+_LIB_PATH = Path(__file__).resolve().parent / (
+    "libtopo_b200_dbg.so" if os.environ.get("TOPO_B200_LIB") == "dbg" else "libtopo_b200.so")
 _lib = None
 
 F64, F32, BF16, BF16_F32IN = 0, 1, 2, 3
@@ -34,6 +38,7 @@ SIGNATURES = {
     "topo_matvec": (_i, [_vp, _i, _vp, _vp, _vp, _vp]),
     "topo_level0_apply": (_i, [_vp, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _d, _d, _d, _d, _vp]),
     "topo_debug_tc_wait": (_i, [_i, _i]),
+    "topo_debug_bounds": (_i, [C.POINTER(_i)]),
     "topo_diag": (_i, [_vp, _vp, _vp, _vp]),
     "topo_gmg_setup": (_i, [_vp, _vp, _vp]),
     "topo_gmg_apply": (_i, [_vp, _vp, _vp, _vp]),

@@ -240,7 +240,8 @@ k_stencil(Grid g, const TC* __restrict__ S, const T* __restrict__ u, const uint8
   T a0 = 0, a1 = 0, a2 = 0;
 #pragma unroll
   for (int k = 0; k < 27; ++k) {
-    const long long j = rb[k / 3] + jzs[k % 3];
+    long long j = rb[k / 3] + jzs[k % 3];
+    if (!topo_in_range(j, g.nnodes)) j = n;
     T uj[3];
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
@@ -258,6 +259,7 @@ k_stencil(Grid g, const TC* __restrict__ S, const T* __restrict__ u, const uint8
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
     const long long i = 3 * n + c;
+    if (!topo_in_range(i, g.ndof)) continue;
     epilogue_store<T, EPI>(ep, i, mask[i] != 0, acc[c], u[i]);
   }
 }
@@ -396,6 +398,7 @@ __global__ void k_restrict(Grid f, Grid c, const T* __restrict__ rf, const uint8
         if (wz == (T)0) continue;
         const T w = wx * wy * wz;
         const long long i = ((long long)ix * f.NY + iy) * f.NZ + iz;
+        if (!topo_in_range(i, f.nnodes)) continue;
         a[0] += w * rf[3 * i];
         a[1] += w * rf[3 * i + 1];
         a[2] += w * rf[3 * i + 2];
@@ -437,6 +440,7 @@ __global__ void k_prolong_add(Grid f, Grid c, const T* __restrict__ ec, const ui
       for (int Jz = pz0; Jz <= min(pz1, c.nz); ++Jz) {
         const T w = wx * wy * (T)prolong_w1(iz, Jz, c.nz);
         const long long J = ((long long)Jx * c.NY + Jy) * c.NZ + Jz;
+        if (!topo_in_range(J, c.nnodes)) continue;
         a[0] += w * ec[3 * J];
         a[1] += w * ec[3 * J + 1];
         a[2] += w * ec[3 * J + 2];
@@ -461,5 +465,7 @@ void prolong_add(bool vec64, const Grid& fine, const Grid& coarse, const void* e
     k_prolong_add<float><<<nb, bs, 0, s>>>(fine, coarse, (const float*)ec, mf, (float*)xf, (float*)e_out, st);
   TOPO_LAUNCH_CHECK();
 }
+
+TOPO_BOUNDS_READER(bounds_flag_coarse)
 
 }  // namespace topo

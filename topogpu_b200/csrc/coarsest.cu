@@ -430,6 +430,7 @@ constexpr int AT = 256;
 
 struct ApplyPlan {
   int nb;
+  long long nfull;       // length of the full vectors rhs and x
   const int* boff;       // nb+1
   const int* link;       // link[b] = 1: block b couples to b-1
   const long long* dioff;  // Di_b, m_b x m_b
@@ -462,7 +463,10 @@ __global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(AT)
     const TX* D = DI + P.dioff[b];
     for (int i = gw; i < m; i += nw) {
       double acc = 0.0;
-      for (int j = lane; j <= i; j += 32) acc += (double)D[(long long)i * m + j] * (double)rhs[free_list[o + j]];
+      for (int j = lane; j <= i; j += 32) {
+        const int f = free_list[o + j];
+        if (topo_in_range(f, P.nfull)) acc += (double)D[(long long)i * m + j] * (double)rhs[f];
+      }
       acc = warp_sum(acc);
       if (lane == 0) y[o + i] = acc;
     }
@@ -514,7 +518,10 @@ __global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(AT)
     cluster_sync();
   }
   // 5. scatter
-  for (int i = rank * AT + threadIdx.x; i < n; i += CL * AT) x[free_list[i]] = (T)__ldcg(z + i);
+  for (int i = rank * AT + threadIdx.x; i < n; i += CL * AT) {
+    const int f = free_list[i];
+    if (topo_in_range(f, P.nfull)) x[f] = (T)__ldcg(z + i);
+  }
 }
 
 }  // namespace cst
@@ -523,6 +530,7 @@ __global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(AT)
 CoarsestPlan coarsest_plan(const Grid& g, const std::vector<int>& free_list) {
   CoarsestPlan p;
   p.n = (int)free_list.size();
+  p.nfull = g.ndof;
   // plane of a compact DoF: node = dof/3, plane = node / (NY*NZ)
   const long long plane_nodes = (long long)g.NY * g.NZ;
   std::vector<int> plane_of(p.n);
@@ -723,6 +731,7 @@ void coarsest_apply(const CoarsestFactor& f, bool vec64, const void* rhs, double
   if (p.n == 0) return;
   cst::ApplyPlan ap;
   ap.nb = p.nb;
+  ap.nfull = p.nfull;
   ap.boff = f.d_boff;
   ap.link = f.d_link;
   ap.dioff = f.d_dioff;
@@ -741,5 +750,7 @@ void coarsest_apply(const CoarsestFactor& f, bool vec64, const void* rhs, double
   }
   TOPO_LAUNCH_CHECK();
 }
+
+TOPO_BOUNDS_READER(bounds_flag_coarsest)
 
 }  // namespace topo

@@ -1372,6 +1372,22 @@ int topo_level0_apply(topo_ctx* c, int u_dtype, int epi, const void* u, const vo
   }
 }
 
+int topo_debug_bounds(int* tripped) {
+  try {
+    if (!tripped) throw std::invalid_argument("topo_debug_bounds: null pointer");
+    const int t = bounds_flag_level0() | bounds_flag_xs() | bounds_flag_cc() | bounds_flag_coarse() |
+                  bounds_flag_coarsest() | bounds_flag_design();
+    *tripped = t ? 1 : 0;
+#ifdef TOPO_DEBUG_BOUNDS
+    return 0;
+#else
+    return 1;
+#endif
+  } catch (const std::exception& e) {
+    return fail(nullptr, e);
+  }
+}
+
 int topo_debug_tc_wait(int skip_first_arrival, int poll_limit) {
   xs_debug(skip_first_arrival, poll_limit);
   return 0;

@@ -76,13 +76,16 @@ __global__ void k_filter(Grid g, int noff, const int* __restrict__ fo, const dou
     for (int k = 0; k < noff; ++k) {
       const int x = ex + fo[3 * k], y = ey + fo[3 * k + 1], z = ez + fo[3 * k + 2];
       if (x < 0 || x >= g.nx || y < 0 || y >= g.ny || z < 0 || z >= g.nz) continue;
-      acc += (fw[k] / hs) * in[((long long)x * g.ny + y) * g.nz + z];
+      const long long j = ((long long)x * g.ny + y) * g.nz + z;
+      if (!topo_in_range(j, g.nelem)) continue;
+      acc += (fw[k] / hs) * in[j];
     }
   } else {
     for (int k = 0; k < noff; ++k) {
       const int x = ex + fo[3 * k], y = ey + fo[3 * k + 1], z = ez + fo[3 * k + 2];
       if (x < 0 || x >= g.nx || y < 0 || y >= g.ny || z < 0 || z >= g.nz) continue;
       const long long i = ((long long)x * g.ny + y) * g.nz + z;
+      if (!topo_in_range(i, g.nelem)) continue;
       acc += (fw[k] / Hs[i]) * in[i];
     }
   }
@@ -446,5 +449,7 @@ void field_stats(long long n, const double* x, double* out4_dev, RedWork red, cu
   k_stats<<<nb, kRedThreads, 0, s>>>(n, x, out4_dev, red);
   TOPO_LAUNCH_CHECK();
 }
+
+TOPO_BOUNDS_READER(bounds_flag_design)
 
 }  // namespace topo

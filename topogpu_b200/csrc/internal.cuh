@@ -251,6 +251,7 @@ void prolong_add(bool vec64, const Grid& fine, const Grid& coarse, const void* e
 // block sweeps over its x-plane blocks. Compact DoF i -> full DoF free[i].
 struct CoarsestPlan {
   int n = 0, nb = 0, mmax = 0;
+  long long nfull = 0;                      // DoFs of the full coarsest-level vectors
   std::vector<int> boff, link;              // block b = compact rows [boff[b], boff[b+1]); link[b]: couples to b-1
   std::vector<long long> dioff, moff, noff; // offsets of Di_b, M_b (and L_{b,b-1}), N_b
   long long di_size = 0, m_size = 0, n_size = 0;
@@ -372,3 +373,43 @@ long long launch_count();
     topo::count_launches(1);     \
     TOPO_CUDA_CHECK(cudaGetLastError()); \
   } while (0)
+
+// ------------------------------------------------ index range-check build
+// Built with -DTOPO_DEBUG_BOUNDS (python -m topogpu_b200.build
+// --debug-bounds -> libtopo_b200_dbg.so), every checked gather/scatter index
+// is tested before the access; an index out of range skips the access and
+// raises a device flag (one per translation unit) that topo_debug_bounds
+// reads back as a status. No trap, no assert. In the normal build the check
+// is the constant true and compiles away.
+#ifdef TOPO_DEBUG_BOUNDS
+static __device__ int g_topo_bounds_flag;
+__device__ __forceinline__ bool topo_in_range(long long i, long long n) {
+  if (i >= 0 && i < n) return true;
+  atomicExch(&g_topo_bounds_flag, 1);
+  return false;
+}
+#define TOPO_BOUNDS_READER(name)                                                   \
+  int name() {                                                                     \
+    int h = 0;                                                                     \
+    TOPO_CUDA_CHECK(cudaMemcpyFromSymbol(&h, g_topo_bounds_flag, sizeof(int)));  \
+    if (h) {                                                                       \
+      const int z = 0;                                                             \
+      TOPO_CUDA_CHECK(cudaMemcpyToSymbol(g_topo_bounds_flag, &z, sizeof(int)));  \
+    }                                                                              \
+    return h;                                                                      \
+  }
+#else
+__device__ __forceinline__ constexpr bool topo_in_range(long long, long long) { return true; }
+#define TOPO_BOUNDS_READER(name) \
+  int name() { return 0; }
+#endif
+
+namespace topo {
+// per translation unit: read and clear its range-check flag (0 in the normal build)
+int bounds_flag_level0();
+int bounds_flag_xs();
+int bounds_flag_cc();
+int bounds_flag_coarse();
+int bounds_flag_coarsest();
+int bounds_flag_design();
+}  // namespace topo

@@ -360,6 +360,7 @@ __global__ void __launch_bounds__(NT) k_level0_cc(const Params<T> P) {
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
           const long long i = 3 * node + c;
+          if (!topo_in_range(i, g.ndof)) continue;
           const bool fr = P.mask[i] != 0;
           if constexpr (EPI == Epi::StoreDot) {
             const T v = fr ? acc[c] : (T)0;
@@ -509,5 +510,7 @@ void level0_apply_cc(bool f64, const Grid& g, const void* u, const void* E, cons
   }
 #undef TOPO_CC_CASE
 }
+
+TOPO_BOUNDS_READER(bounds_flag_cc)
 
 }  // namespace topo

@@ -638,6 +638,7 @@ __global__ void __launch_bounds__(NT, 1) k_level0_xs(const Params<TU> P) {
 #pragma unroll
             for (int cc = 0; cc < 3; ++cc) {
               const long long i = row_dof + 3 * z + cc;
+              if (!topo_in_range(i, g.ndof)) continue;
               const int li = lrow + 3 * z + cc;
               const bool fr = (mw >> cc) & 1;
               const float acc = out[3 * tn + cc];
@@ -918,5 +919,7 @@ void xs_debug(int skip_first_arrival, int poll_limit) {
   g_xs_skip = skip_first_arrival ? 1 : 0;
   g_xs_poll = poll_limit > 0 ? poll_limit : (1 << 22);
 }
+
+TOPO_BOUNDS_READER(bounds_flag_xs)
 
 }  // namespace topo

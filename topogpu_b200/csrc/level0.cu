@@ -194,6 +194,7 @@ k_level0(Grid g, const TU* __restrict__ u, const T* __restrict__ E, const uint8_
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
         const long long i = 3 * node + c;
+        if (!topo_in_range(i, g.ndof)) continue;
         const T v = mask[i] ? (T)acc[c] : (T)0;
         ep.y[i] = v;
         part[0] += (double)load_as<TS>(u + i) * (double)v;
@@ -212,6 +213,7 @@ k_level0(Grid g, const TU* __restrict__ u, const T* __restrict__ E, const uint8_
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
     const long long i = 3 * node + c;
+    if (!topo_in_range(i, g.ndof)) continue;
     epilogue_store<T, EPI>(ep, i, mask[i] != 0, (T)acc[c], load_as<T>(u + i));
   }
 }
@@ -335,7 +337,8 @@ __global__ void k_sensitivity(Grid g, const TU* __restrict__ u, const TU* __rest
     const int bx = (m == 1 || m == 2 || m == 5 || m == 6);
     const int by = (m == 2 || m == 3 || m == 6 || m == 7);
     const int bz = (m >= 4);
-    const long long n = ((long long)(ex + bx) * g.NY + (ey + by)) * g.NZ + (ez + bz);
+    long long n = ((long long)(ex + bx) * g.NY + (ey + by)) * g.NZ + (ez + bz);
+    if (!topo_in_range(n, g.nnodes)) n = 0;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       ue[3 * m + c] = (double)u[3 * n + c];
@@ -385,5 +388,7 @@ void sensitivity(const Grid& g, const void* u, const void* v, bool u_f32, const 
     k_sensitivity<double><<<nb, bs, 0, s>>>(g, (const double*)u, (const double*)v, rho, penal, E0, Emin, dc);
   TOPO_LAUNCH_CHECK();
 }
+
+TOPO_BOUNDS_READER(bounds_flag_level0)
 
 }  // namespace topo
