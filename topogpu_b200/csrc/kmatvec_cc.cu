@@ -418,7 +418,9 @@ CcDevice& cc_device() {
   return d;
 }
 
-constexpr int kCcSmemMax = 232448;
+// the opt-in limit covers static and dynamic shared memory together; the
+// kernel's static part (abort flag, reduction scratch) stays under 2 KB
+constexpr int kCcSmemMax = 232448 - 2048;
 int al128(long long x) { return (int)((x + 127) & ~127LL); }
 
 struct CcLayout {
