@@ -123,12 +123,24 @@ int topo_level0_apply(topo_ctx* ctx, int u_dtype, int epi, const void* u, const 
                       void* r, void* x, void* d_out, const void* dinv, double s, double c1, double c2, double ax,
                       void* stream);
 
-/* Test hook for the bounded waits of the tensor-core K.u (no reference
- * counterpart): with skip_first_arrival != 0 the kernel's converter warps
- * withhold their first arrival, so its MMA role's wait runs out after
- * poll_limit polls (<= 0: the default limit); the kernel then raises its
- * error flag, drains and exits, and the entry point that launched it
- * returns an error. Applies to later launches in this process. */
+/* Bounded waits (no reference counterpart). Every mbarrier wait of the
+ * streaming level-0 kernels gives up after a poll limit, raises a per-device
+ * flag in mapped host memory, drains its copies in flight and exits. The
+ * asynchronous entries (topo_matvec, topo_level0_apply, topo_gmg_apply)
+ * report a flag raised by an earlier launch that has finished, before they
+ * launch; topo_pcg / topo_solve and topo_wait_status synchronise and report
+ * it at once. The flag is cleared when reported. */
+
+/* Synchronises the context's stream (stream != NULL: that stream) and
+ * returns nonzero, with the message in topo_last_error, when a wait of a
+ * level-0 kernel launched before it timed out. */
+int topo_wait_status(topo_ctx* ctx, void* stream);
+
+/* Test hook for the bounded waits: with skip_first_arrival != 0 the
+ * tensor-core K.u's converter warps withhold their first arrival, so its
+ * MMA role's wait runs out after poll_limit polls (<= 0: the default limit)
+ * and the kernel raises the flag. Applies to later launches in this
+ * process. */
 int topo_debug_tc_wait(int skip_first_arrival, int poll_limit);
 
 /* Index range checks (no reference counterpart). In the library built with

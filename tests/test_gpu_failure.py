@@ -50,10 +50,16 @@ def test_tensor_core_wait_timeout_returns_error(cuda_dev):
     ub = torch.tensor(u, device=DEV).to(torch.bfloat16)
     assert lib.topo_debug_tc_wait(1, 1 << 14) == 0
     try:
+        ctx.level0_apply(ub, Et, "store")  # asynchronous: returns before the wait runs out
         with pytest.raises(RuntimeError, match="timed out"):
-            ctx.level0_apply(ub, Et, "store")
+            ctx.wait_status()
+        ctx.level0_apply(ub, Et, "store")
+        torch.cuda.synchronize()
     finally:
         lib.topo_debug_tc_wait(0, 0)
+    # a later asynchronous call reports the earlier launch's timeout before launching
+    with pytest.raises(RuntimeError, match="earlier launch timed out"):
+        ctx.level0_apply(ub, Et, "store")
     # the context and the device are still usable, and the error flag was cleared
     y = ctx.level0_apply(ub, Et, "store").cpu().numpy()
     ref = fem.matvec_full(fem.bf16_round(u), E, nel, "bf16").astype(np.float64)

@@ -37,6 +37,7 @@ SIGNATURES = {
     "topo_modulus": (_i, [_vp, _vp, _d, _d, _d, _vp, _vp]),
     "topo_matvec": (_i, [_vp, _i, _vp, _vp, _vp, _vp]),
     "topo_level0_apply": (_i, [_vp, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _d, _d, _d, _d, _vp]),
+    "topo_wait_status": (_i, [_vp, _vp]),
     "topo_debug_tc_wait": (_i, [_i, _i]),
     "topo_debug_bounds": (_i, [C.POINTER(_i)]),
     "topo_diag": (_i, [_vp, _vp, _vp, _vp]),

@@ -118,6 +118,11 @@ class TopoContext:
     EPILOGUES = {"store": _lib.EPI_STORE, "residual": _lib.EPI_RESIDUAL, "rupd": _lib.EPI_RUPD,
                  "cheb": _lib.EPI_CHEB}
 
+    def wait_status(self):
+        """Synchronise and raise if a wait of an earlier level-0 launch timed
+        out (asynchronous entries report it only at their next call)."""
+        self._chk(self._lib.topo_wait_status(self._h, _stream()), "wait_status")
+
     def level0_apply(self, u, E, epi="store", *, y=None, b=None, r=None, x=None, d_out=None, dinv=None, s=1.0,
                      c1=0.0, c2=0.0, ax=0.0, u_fp32_to_bf16=False):
         """One level-0 operator application with its fused epilogue (see

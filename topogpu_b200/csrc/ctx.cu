@@ -362,6 +362,40 @@ void vcycle_apply(topo_ctx* c, const void* r, void* z, const KrylovState* st, cu
 }
 
 // ------------------------------------------------------- spectral bounds
+// The power iterations keep their scalars on the device (dot products into
+// dtmp, normalisations by kernels that read them) and read lambda back once
+// at the end: no host round trip per iteration.
+
+// y = x / sqrt(*s2) when *s2 > 0 (y keeps its value otherwise)
+template <typename T>
+__global__ void k_scale_rsqrt(long long n, const T* __restrict__ x, const double* s2, T* __restrict__ y) {
+  const double q = *s2;
+  if (!(q > 0.0)) return;
+  const T f = (T)(1.0 / sqrt(q));
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    y[i] = f * x[i];
+}
+
+// Keep the iteration's Rayleigh quotient parts (num, den) when its update
+// norm is non-zero (the reference stops before a zero-norm update).
+__global__ void k_commit_lambda(double* d) {
+  if (d[2] > 0.0) {
+    d[3] = d[1];
+    d[4] = d[0];
+  }
+}
+
+__global__ void k_set2(double* d, double a, double b) {
+  d[3] = a;
+  d[4] = b;
+}
+
+template <typename T>
+static void scale_rsqrt(long long n, const void* x, const double* s2, void* y, cudaStream_t s) {
+  k_scale_rsqrt<T><<<gblocks(n), 256, 0, s>>>(n, (const T*)x, s2, (T*)y);
+  TOPO_LAUNCH_CHECK();
+}
+
 // lambda_max(D^-1 K) on level 0 by D-norm power iteration (multigrid_v4.py:273-295).
 double lambda_fine(topo_ctx* c, cudaStream_t s) {
   Level& L0 = c->L[0];
@@ -370,38 +404,38 @@ double lambda_fine(topo_ctx* c, cudaStream_t s) {
   void* v = L0.x;
   void* Kv = L0.r;
   void* Av = L0.d2;
-  double* d = c->dtmp;
+  double* d = c->dtmp;  // d[0] v^T D v, d[1] v^T K v, d[2] |D^-1 K v|_D^2
   const int rnd = c->cheb_form == 1;
   if (f64) k_mask_to<double><<<gblocks(n), 256, 0, s>>>(n, L0.mask, (double*)v, rnd);
   else k_mask_to<float><<<gblocks(n), 256, 0, s>>>(n, L0.mask, (float*)v, rnd);
   TOPO_LAUNCH_CHECK();
-  auto dotdiv = [&](const void* a, const void* b) {
-    if (f64) k_dot_div<double><<<kRedBlocks, kRedThreads, 0, s>>>(n, (const double*)a, (const double*)b, (const double*)L0.dinv, d, c->red);
-    else k_dot_div<float><<<kRedBlocks, kRedThreads, 0, s>>>(n, (const float*)a, (const float*)b, (const float*)L0.dinv, d, c->red);
+  auto dotdiv = [&](const void* a, const void* b, double* out) {
+    if (f64) k_dot_div<double><<<kRedBlocks, kRedThreads, 0, s>>>(n, (const double*)a, (const double*)b, (const double*)L0.dinv, out, c->red);
+    else k_dot_div<float><<<kRedBlocks, kRedThreads, 0, s>>>(n, (const float*)a, (const float*)b, (const float*)L0.dinv, out, c->red);
     TOPO_LAUNCH_CHECK();
-    double h;
-    TOPO_CUDA_CHECK(cudaMemcpyAsync(&h, d, sizeof(double), cudaMemcpyDeviceToHost, s));
-    TOPO_CUDA_CHECK(cudaStreamSynchronize(s));
-    return h;
   };
-  double vDv = dotdiv(v, v);
-  axpby(f64, n, 1.0 / std::sqrt(vDv), v, 0.0, v, s);
-  double lam = 1.0;
+  auto rs = [&](const void* x, const double* s2, void* y) {
+    if (f64) scale_rsqrt<double>(n, x, s2, y, s);
+    else scale_rsqrt<float>(n, x, s2, y, s);
+  };
+  dotdiv(v, v, d);
+  rs(v, d, v);
   const Prec p = f64 ? Prec::F64 : Prec::F32;
   for (int it = 0; it < 20; ++it) {
     EpiArgs ea{};
     level0_apply(p, L0.g, v, f64 ? (const void*)c->E64 : (const void*)c->E32, L0.mask, Kv, Epi::Store, ea, s);
-    vDv = dotdiv(v, v);
-    const double vKv = dot_host(f64, n, v, Kv, c->red, d, s);
-    lam = vKv / std::max(vDv, 1e-300);
+    dotdiv(v, v, d);
+    dot_to(f64, n, v, Kv, d + 1, c->red, s);
     if (f64) k_hadamard<double><<<gblocks(n), 256, 0, s>>>(n, (const double*)L0.dinv, (const double*)Kv, (double*)Av);
     else k_hadamard<float><<<gblocks(n), 256, 0, s>>>(n, (const float*)L0.dinv, (const float*)Kv, (float*)Av);
     TOPO_LAUNCH_CHECK();
-    const double nrm = std::sqrt(dotdiv(Av, Av));
-    if (nrm <= 1e-300) break;
-    axpby(f64, n, 1.0 / nrm, Av, 0.0, v, s);
+    dotdiv(Av, Av, d + 2);
+    rs(Av, d + 2, v);
   }
-  return lam;
+  double h[2];
+  TOPO_CUDA_CHECK(cudaMemcpyAsync(h, d, sizeof(h), cudaMemcpyDeviceToHost, s));
+  TOPO_CUDA_CHECK(cudaStreamSynchronize(s));
+  return h[1] / std::max(h[0], 1e-300);
 }
 
 // Coarse level power iteration (multigrid_v4.py:298-314), FP64 stencil.
@@ -411,29 +445,30 @@ double lambda_coarse(topo_ctx* c, int l, double* dinv64, cudaStream_t s) {
   double* V = c->C.scrA;
   double* KV = c->C.scrB;
   double* AV = c->C.scrC;
+  double* d = c->dtmp;  // d[0] v^T D v, d[1] v^T K v, d[2] |D^-1 K v|^2, d[3]/d[4] the kept quotient
   k_mask_to<double><<<gblocks(n), 256, 0, s>>>(n, Lv.mask, V, c->cheb_form == 1);
   TOPO_LAUNCH_CHECK();
-  double* d = c->dtmp;
-  double nrm0 = std::sqrt(dot_host(true, n, V, V, c->red, d, s));
-  axpby(true, n, 1.0 / nrm0, V, 0.0, V, s);
-  double lam = 1.0;
+  k_set2<<<1, 1, 0, s>>>(d, 1.0, 1.0);  // lambda 1 if the first update is zero
+  TOPO_LAUNCH_CHECK();
+  dot_to(true, n, V, V, d + 2, c->red, s);
+  scale_rsqrt<double>(n, V, d + 2, V, s);
   for (int it = 0; it < 10; ++it) {
     EpiArgs ea{};
     stencil_apply(Prec::F64, true, Lv.g, Lv.S64, V, Lv.mask, KV, Epi::Store, ea, s);
     k_hadamard<double><<<gblocks(n), 256, 0, s>>>(n, dinv64, KV, AV);
     TOPO_LAUNCH_CHECK();
-    const double nrm = std::sqrt(dot_host(true, n, AV, AV, c->red, d, s));
-    if (nrm <= 1e-300) break;
-    const double vKv = dot_host(true, n, V, KV, c->red, d, s);
+    dot_to(true, n, AV, AV, d + 2, c->red, s);
+    dot_to(true, n, V, KV, d + 1, c->red, s);
     k_dot_div<double><<<kRedBlocks, kRedThreads, 0, s>>>(n, V, V, dinv64, d, c->red);
     TOPO_LAUNCH_CHECK();
-    double vDv;
-    TOPO_CUDA_CHECK(cudaMemcpyAsync(&vDv, d, sizeof(double), cudaMemcpyDeviceToHost, s));
-    TOPO_CUDA_CHECK(cudaStreamSynchronize(s));
-    lam = vKv / std::max(vDv, 1e-300);
-    axpby(true, n, 1.0 / nrm, AV, 0.0, V, s);
+    k_commit_lambda<<<1, 1, 0, s>>>(d);
+    TOPO_LAUNCH_CHECK();
+    scale_rsqrt<double>(n, AV, d + 2, V, s);
   }
-  return std::max(lam, 1e-6);
+  double h[2];
+  TOPO_CUDA_CHECK(cudaMemcpyAsync(h, d + 3, sizeof(h), cudaMemcpyDeviceToHost, s));
+  TOPO_CUDA_CHECK(cudaStreamSynchronize(s));
+  return std::max(h[0] / std::max(h[1], 1e-300), 1e-6);
 }
 
 // --------------------------------------------------------------- setup
@@ -729,12 +764,11 @@ int do_pcg(topo_ctx* c, const double* b, double* x, double tol, int maxiter, int
     ++refreshes;
   }
   rr = true_residual(c, s);
-  if (c->use_tc && xs_error_flag(s)) throw std::runtime_error("tensor-core K.u: an mbarrier wait timed out");
+  if (xs_error_flag(s)) throw std::runtime_error("level-0 K.u: an mbarrier wait timed out");
   if (!std::isfinite(rr)) throw std::runtime_error("topo_pcg: the iteration produced NaN or Inf");
   TOPO_CUDA_CHECK(cudaMemcpyAsync(x, c->kx64, vb, cudaMemcpyDeviceToDevice, s));
   if (out_iters) *out_iters = iters;
   if (out_relres) *out_relres = bb > 0 ? std::sqrt(rr / bb) : 0.0;
-  if (c->use_tc && xs_error_flag(s)) throw std::runtime_error("tensor-core K.u: an mbarrier wait timed out");
   return converged ? 0 : 1;
 }
 
@@ -1041,6 +1075,7 @@ static void register_ke(topo_ctx* c, const double* KE) {
           "(KE is held in constant memory shared by all contexts of a device)");
   } else {
     set_ke(KE);
+    cc_set_ke(KE);
     set_ke_block(KE);
     std::vector<double> Q(8 * 576);
     host_galerkin_q(KE, Q.data());
@@ -1298,6 +1333,8 @@ int topo_matvec(topo_ctx* c, int dtype, const void* u, void* y, const void* E, v
     if (!c || !u || !y || !E) throw std::invalid_argument("topo_matvec: null pointer");
     if (!c->problem_set) throw std::runtime_error("topo_matvec: call topo_set_problem first");
     StreamGuard sg(c, stream);
+    if (xs_error_flag(c->cs, false))
+      throw std::runtime_error("level-0 K.u: an mbarrier wait of an earlier launch timed out");
     Level& L0 = c->L[0];
     EpiArgs ea{};
     if (dtype == TOPO_F64) level0_apply(Prec::F64, L0.g, u, E, L0.mask, y, Epi::Store, ea, c->cs);
@@ -1305,7 +1342,6 @@ int topo_matvec(topo_ctx* c, int dtype, const void* u, void* y, const void* E, v
     else if (dtype == TOPO_BF16) {
       if (c->use_tc && level0_xs_supported(L0.g)) {
         level0_apply_xs(true, L0.g, u, E, c->nmask0, y, Epi::Store, ea, c->cs);
-        if (xs_error_flag(c->cs)) throw std::runtime_error("tensor-core K.u: an mbarrier wait timed out");
       } else {
         level0_apply_bf16_input(L0.g, u, E, L0.mask, y, c->cs);
       }
@@ -1339,6 +1375,8 @@ int topo_level0_apply(topo_ctx* c, int u_dtype, int epi, const void* u, const vo
       default: throw std::invalid_argument("topo_level0_apply: bad epilogue");
     }
     StreamGuard sg(c, stream);
+    if (xs_error_flag(c->cs, false))
+      throw std::runtime_error("level-0 K.u: an mbarrier wait of an earlier launch timed out");
     Level& L0 = c->L[0];
     EpiArgs ea{};
     ea.b = b;
@@ -1356,7 +1394,6 @@ int topo_level0_apply(topo_ctx* c, int u_dtype, int epi, const void* u, const vo
       const bool u16 = u_dtype == TOPO_BF16;
       if (c->use_tc && level0_xs_supported(L0.g)) {
         level0_apply_xs(u16, L0.g, u, E, c->nmask0, y, ep, ea, c->cs);
-        if (xs_error_flag(c->cs)) throw std::runtime_error("tensor-core K.u: an mbarrier wait timed out");
       } else if (!u16) {
         level0_apply(Prec::BF16, L0.g, u, E, L0.mask, y, ep, ea, c->cs);
       } else {
@@ -1366,6 +1403,17 @@ int topo_level0_apply(topo_ctx* c, int u_dtype, int epi, const void* u, const vo
     } else {
       throw std::invalid_argument("topo_level0_apply: bad dtype");
     }
+    return 0;
+  } catch (const std::exception& e) {
+    return fail(c, e);
+  }
+}
+
+int topo_wait_status(topo_ctx* c, void* stream) {
+  try {
+    if (!c) throw std::invalid_argument("topo_wait_status: null context");
+    StreamGuard sg(c, stream);
+    if (xs_error_flag(c->cs, true)) throw std::runtime_error("level-0 K.u: an mbarrier wait timed out");
     return 0;
   } catch (const std::exception& e) {
     return fail(c, e);
@@ -1422,8 +1470,9 @@ int topo_gmg_apply(topo_ctx* c, const void* r, void* z, void* stream) {
     if (!c || !r || !z) throw std::invalid_argument("topo_gmg_apply: null pointer");
     if (!c->setup_done) throw std::runtime_error("topo_gmg_apply: call topo_gmg_setup first");
     StreamGuard sg(c, stream);
+    if (xs_error_flag(c->cs, false))
+      throw std::runtime_error("level-0 K.u: an mbarrier wait of an earlier launch timed out");
     vcycle_apply(c, r, z, nullptr, c->cs);
-    if (c->use_tc && xs_error_flag(c->cs)) throw std::runtime_error("tensor-core K.u: an mbarrier wait timed out");
     return 0;
   } catch (const std::exception& e) {
     return fail(c, e);

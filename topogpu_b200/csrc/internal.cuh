@@ -217,9 +217,10 @@ bool level0_xs_supported(const Grid& g);
 // nmask: per-node free bits (bit c = DoF 3n+c free)
 void level0_apply_xs(bool u_bf16, const Grid& g, const void* u, const void* E, const uint8_t* nmask, void* y, Epi epi,
                      const EpiArgs& ea, cudaStream_t s);
-int xs_error_flag(cudaStream_t s);
+int xs_error_flag(cudaStream_t s, bool sync = true);
 int* wait_error_flag();
 // FP32 / FP64 level-0 K.u on the CUDA cores streaming along x (kmatvec_cc.cu)
+void cc_set_ke(const double* KE_host);
 bool level0_cc_supported(const Grid& g, bool f64);
 void level0_apply_cc(bool f64, const Grid& g, const void* u, const void* E, const uint8_t* mask, void* y, Epi epi,
                      const EpiArgs& ea, int* err, cudaStream_t s);

@@ -28,10 +28,13 @@
 
 namespace topo {
 
-extern __constant__ double cKE64[576];
-extern __constant__ float cKE32[576];
-
 namespace cc {
+
+// KE in this file's own constant bank (the library is built without
+// relocatable device code, so constants cannot be shared across files; the
+// per-device upload is cc_set_ke, called with the other KE copies).
+__constant__ double cKE64[576];
+__constant__ float cKE32[576];
 
 constexpr int NCW = 8;            // compute warps
 constexpr int NT = 32 * (NCW + 1);
@@ -105,7 +108,8 @@ __device__ __forceinline__ bool wait_bar(uint32_t bar, uint32_t parity, volatile
     if ((it & 63) == 63 && *abort_flag) return false;
   }
   *abort_flag = 1;
-  atomicExch(err, 1);
+  *(volatile int*)err = 1;  // mapped host memory: readable without a device sync
+  __threadfence_system();
   return false;
 }
 
@@ -486,6 +490,13 @@ void launch_cc(const Grid& g, const void* u, const void* E, const uint8_t* mask,
   TOPO_LAUNCH_CHECK();
 }
 }  // namespace
+
+void cc_set_ke(const double* KE) {
+  float f[576];
+  for (int i = 0; i < 576; ++i) f[i] = (float)KE[i];
+  TOPO_CUDA_CHECK(cudaMemcpyToSymbol(cc::cKE64, KE, sizeof(double) * 576));
+  TOPO_CUDA_CHECK(cudaMemcpyToSymbol(cc::cKE32, f, sizeof(float) * 576));
+}
 
 bool level0_cc_supported(const Grid& g, bool f64) {
   CcLayout L;

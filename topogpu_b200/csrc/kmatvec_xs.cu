@@ -182,7 +182,8 @@ __device__ __forceinline__ bool wait_bar(uint32_t bar, uint32_t parity, volatile
     if ((it & 63) == 63 && *abort_flag) return false;
   }
   *abort_flag = 1;
-  atomicExch(err, 1);
+  *(volatile int*)err = 1;  // mapped host memory: readable without a device sync
+  __threadfence_system();
   return false;
 }
 
@@ -704,7 +705,8 @@ namespace topo {
 namespace {
 struct XsDevice {
   __nv_bfloat16* B = nullptr;
-  int* err = nullptr;
+  int* err = nullptr;       // device alias of err_host
+  int* err_host = nullptr;
   int nsm = 0;
   uint32_t attr_done = 0;  // bit per kernel instance
 };
@@ -865,8 +867,11 @@ void xs_prepare(const double* KE) {
   XsDevice& d = xs_device();
   if (!d.B) TOPO_CUDA_CHECK(cudaMalloc(&d.B, sizeof(h)));
   if (!d.err) {
-    TOPO_CUDA_CHECK(cudaMalloc(&d.err, sizeof(int)));
-    TOPO_CUDA_CHECK(cudaMemset(d.err, 0, sizeof(int)));
+    // Pinned, mapped host word: kernels store 1 through the device alias and
+    // the host reads it without synchronising the stream.
+    TOPO_CUDA_CHECK(cudaHostAlloc(&d.err_host, sizeof(int), cudaHostAllocMapped | cudaHostAllocPortable));
+    *(volatile int*)d.err_host = 0;
+    TOPO_CUDA_CHECK(cudaHostGetDevicePointer((void**)&d.err, d.err_host, 0));
   }
   TOPO_CUDA_CHECK(cudaMemcpy(d.B, h, sizeof(h), cudaMemcpyHostToDevice));
 }
@@ -895,14 +900,16 @@ void level0_apply_xs(bool u_bf16, const Grid& g, const void* u, const void* E, c
 #undef TOPO_XS_CASE
 }
 
-// Returns and clears this device's flag set when an mbarrier wait timed out.
-int xs_error_flag(cudaStream_t s) {
+// Returns and clears this device's flag, set when an mbarrier wait timed out.
+// sync: wait for the stream first, so launches already queued on it count;
+// otherwise only launches that have finished are seen (no host stall).
+int xs_error_flag(cudaStream_t s, bool sync) {
   XsDevice& d = xs_device();
-  if (!d.err) return 0;
-  int h = 0;
-  TOPO_CUDA_CHECK(cudaMemcpyAsync(&h, d.err, sizeof(int), cudaMemcpyDeviceToHost, s));
-  TOPO_CUDA_CHECK(cudaStreamSynchronize(s));
-  if (h) TOPO_CUDA_CHECK(cudaMemsetAsync(d.err, 0, sizeof(int), s));
+  if (!d.err_host) return 0;
+  if (sync) TOPO_CUDA_CHECK(cudaStreamSynchronize(s));
+  volatile int* f = d.err_host;
+  const int h = *f;
+  if (h) *f = 0;
   return h;
 }
 
