@@ -37,7 +37,9 @@ constexpr int CNB = 32;  // panel width
 
 __device__ __forceinline__ double ldcg(const double* p) { return __ldcg(p); }
 
-// Band storage: row i holds columns i-band .. i at B[i*ldb + (j - i + band)].
+// Band storage: row i holds columns i-band .. i at B[i*ldb + (j - i + band)];
+// every access checks i - j <= band first (the band can be narrower than a
+// 32-wide panel on small coarsest grids).
 __device__ __forceinline__ long long bidx(long long i, long long j, int band, long long ldb) {
   return i * ldb + (j - i + band);
 }
@@ -170,7 +172,8 @@ __global__ void __launch_bounds__(256) k_band_chol(int n, int band, long long ld
     //    same arithmetic, so all agree); identity-padded past n
     for (int q = tid; q < CNB * CNB; q += blockDim.x) {
       const int i = q / CNB, j = q % CNB;
-      S.W[i][j] = (i < nb && j < nb && j <= i) ? ldcg(A + bidx(k + i, k + j, band, ldb)) : (i == j ? 1.0 : 0.0);
+      S.W[i][j] = (i < nb && j < nb && j <= i) ? (i - j <= band ? ldcg(A + bidx(k + i, k + j, band, ldb)) : 0.0)
+                                               : (i == j ? 1.0 : 0.0);
     }
     __syncthreads();
     if (tid < 32) {
@@ -207,7 +210,7 @@ __global__ void __launch_bounds__(256) k_band_chol(int n, int band, long long ld
     if (blockIdx.x == 0) {
       for (int q = tid; q < CNB * CNB; q += blockDim.x) {
         const int i = q / CNB, j = q % CNB;
-        if (i < nb && j <= i) L[bidx(k + i, k + j, band, ldb)] = S.Ld[i][j];
+        if (i < nb && j <= i && i - j <= band) L[bidx(k + i, k + j, band, ldb)] = S.Ld[i][j];
       }
       if (tid == 0 && S.bad) *flag = 1;
     }
@@ -333,8 +336,9 @@ __global__ void __launch_bounds__(256) k_block_inverse(const int* __restrict__ b
     // the diagonal sub-block L_II
     for (int q = tid; q < CNB * CNB; q += blockDim.x) {
       const int rr = q / CNB, kk = q % CNB;
-      S.Lc[rr][kk] = (i0 + rr < m && i0 + kk < m && kk <= rr) ? L[bidx(o + i0 + rr, o + i0 + kk, band, ldb)]
-                                                                : (rr == kk ? 1.0 : 0.0);
+      S.Lc[rr][kk] = (i0 + rr < m && i0 + kk < m && kk <= rr)
+                         ? (rr - kk <= band ? L[bidx(o + i0 + rr, o + i0 + kk, band, ldb)] : 0.0)
+                         : (rr == kk ? 1.0 : 0.0);
     }
     __syncthreads();
     if (tid < CNB) {
