@@ -1,28 +1,29 @@
 // coarsest.cu - direct FP64 solve of the coarsest multigrid level.
 //
 // The coarsest operator (free DoFs only, compact numbering in reference DoF
-// order) couples x-planes only to their neighbours, so in plane blocks it is
-// block tridiagonal and its Cholesky factor L is block bidiagonal: L_bb lower
-// triangular and L_{b,b-1} dense. The setup
-//   1. assembles the lower band (|i-j| <= band) into band storage,
+// order) is banded: a DoF couples only to DoFs of its own and the two
+// neighbouring x-planes, so |i-j| <= band with band about one x-plane of
+// DoFs. The setup
+//   1. assembles the lower band into band storage,
 //   2. factorises it with one persistent kernel: a right-looking band
-//      Cholesky over 32-column panels, one grid barrier per panel (each CTA
-//      factors the panel's diagonal block itself, solves the panel rows of
-//      its trailing tiles and updates them; the factor goes to a separate
-//      band array so no CTA reads a panel row another CTA has overwritten),
-//   3. inverts every diagonal plane block, Di_b = L_bb^-1, and forms
-//      M_b = Di_b L_{b,b-1} and N_b = Di_b^T L_{b+1,b}^T (FP64 arithmetic,
-//      stored in the apply precision).
-// The apply z = K^-1 r is then two sweeps over the plane blocks,
-//   y_b = Di_b r_b - M_b y_{b-1},   z_b = Di_b^T y_b - N_b z_{b+1},
-// run by one thread-block cluster (8 CTAs) with one cluster barrier per
-// block: y and z stay in L2, each block step reads the previous block's
-// values once into shared memory.
+//      Cholesky over 32-column panels with one grid barrier per panel (every
+//      CTA factors the panel's diagonal block in one warp's registers while
+//      two other warps fetch the panel rows of its trailing tile; they solve
+//      them, the CTA updates the tile; the factor goes to a separate band
+//      array so no CTA reads a panel row another CTA has overwritten),
+//   3. inverts the 32x32 diagonal blocks of L and forms W = L^-1 by forward
+//      substitution in independent 16-column strips (W is dense lower
+//      triangular; the band of L bounds each step's reads),
+//   4. stores W (lower triangle) and W^T (strict upper triangle) in one
+//      row-major matrix C in the apply precision.
+// The apply z = K^-1 r = W^T (W r) is two bandwidth-bound passes over C, one
+// warp per row, each reading a row contiguously.
 //
 // Reference: the coarsest solve of GalerkinMatFreeGMG (src/gpu_fem/
 // multigrid_v4.py:774-811, 969-984): dense Cholesky with an eps*I retry when a
-// pivot is not positive. The factor here is the same (a band Cholesky creates
-// no fill outside the band); only the storage and the apply differ.
+// pivot is not positive, and two triangular solves per application. The
+// factor here is the same (a band Cholesky creates no fill outside the band);
+// the triangular solves become products with the explicit inverse.
 #include "internal.cuh"
 #include "reduce.cuh"
 
@@ -120,9 +121,9 @@ __device__ bool grid_barrier(unsigned* count, unsigned* gen, unsigned nblocks, i
 }
 
 // ------------------------------------------------------ persistent Cholesky
-// Shared memory of one CTA: the panel's diagonal block (factored in place by
-// warp 0 into Ld and its reciprocal pivots), and the panel rows of the two
-// row tiles of the trailing tile it updates (solved in place).
+// Shared memory of one CTA: the panel's diagonal block (factored by warp 0
+// into Ld and its reciprocal pivots) and the solved panel rows of the two row
+// tiles of the trailing tile it updates.
 struct CholSmem {
   double W[CNB][CNB + 1];
   double Ld[CNB][CNB + 1];
@@ -139,70 +140,87 @@ __device__ __forceinline__ void tile_of(int t, int& ti, int& tj) {
   tj = t - ti * (ti + 1) / 2;
 }
 
-// Solve rows [r0, r0+32) of the panel (columns k .. k+nb) against the
-// factored diagonal block: X Ld^T = A_panel. Rows past `lim` or entries
-// outside the band are zero. 32 threads, one row each.
-__device__ __forceinline__ void panel_solve(const double* A, int band, long long ldb, int k, int nb, int r0, int lim,
-                                            CholSmem& S, double (*P)[CNB + 1]) {
-  const int t = threadIdx.x;
-  if (t < CNB) {
-    const int i = r0 + t;
-    double x[CNB];
-#pragma unroll
-    for (int j = 0; j < CNB; ++j) x[j] = (i < lim && j < nb && i - (k + j) <= band) ? ldcg(A + bidx(i, k + j, band, ldb)) : 0.0;
-#pragma unroll
-    for (int j = 0; j < CNB; ++j) {
-      x[j] *= S.invd[j];
-#pragma unroll
-      for (int q = j + 1; q < CNB; ++q) x[q] -= x[j] * S.Ld[q][j];
-    }
-#pragma unroll
-    for (int j = 0; j < CNB; ++j) P[t][j] = x[j];
+// One pivot of the warp-register factor of a 32x32 diagonal block (lane =
+// row). The pivot index is a template parameter so that every register index
+// is a compile-time constant (the array stays in registers).
+template <int J>
+__device__ __forceinline__ void chol_step(double (&wr)[CNB], int lane, CholSmem& S, bool& bad) {
+  const double d = __shfl_sync(0xffffffffu, wr[J], J);
+  const bool ok = d > 0.0 && isfinite(d);
+  const double dd = ok ? d : 1.0;
+  const double rs = rsqrt(dd);
+  const double lj = wr[J];
+  if (lane == J) {
+    bad |= !ok;
+    S.Ld[J][J] = dd * rs;
+    S.invd[J] = rs;
+  } else {
+    S.Ld[lane][J] = lane > J ? lj * rs : 0.0;
   }
+  const double w = lj * (rs * rs);
+#pragma unroll
+  for (int t = J + 1; t < CNB; ++t) {
+    const double ct = __shfl_sync(0xffffffffu, wr[J], t);
+    if (t <= lane) wr[t] -= ct * w;
+  }
+  if constexpr (J + 1 < CNB) chol_step<J + 1>(wr, lane, S, bad);
 }
 
-__global__ void __launch_bounds__(256) k_band_chol(int n, int band, long long ldb, double* A, double* L, int* flag,
-                                                   unsigned* bar_count, unsigned* bar_gen, int* err, int poll) {
+// Panel row i (columns k .. k+nb) into registers; zero past `lim` or outside
+// the band.
+__device__ __forceinline__ void panel_load(const double* A, int band, long long ldb, int k, int nb, int i, int lim,
+                                           double (&x)[CNB]) {
+#pragma unroll
+  for (int j = 0; j < CNB; ++j)
+    x[j] = (i < lim && j < nb && i - (k + j) <= band) ? ldcg(A + bidx(i, k + j, band, ldb)) : 0.0;
+}
+
+// x Ld^T = a for one row, column by column with the reciprocal pivots.
+template <int J>
+__device__ __forceinline__ void solve_step(double (&x)[CNB], const CholSmem& S) {
+  x[J] *= S.invd[J];
+#pragma unroll
+  for (int q = J + 1; q < CNB; ++q) x[q] -= x[J] * S.Ld[q][J];
+  if constexpr (J + 1 < CNB) solve_step<J + 1>(x, S);
+}
+
+// Warps: 0 factors the diagonal block, 2 and 3 solve the panel rows of the
+// two row tiles of each trailing tile (3 only for off-diagonal tiles), all
+// 256 threads update the tile (four outputs each). The first tile's panel
+// rows are loaded before the factor, so that load overlaps it.
+__global__ void __launch_bounds__(256, 1) k_band_chol(int n, int band, long long ldb, double* A, double* L, int* flag,
+                                                      unsigned* bar_count, unsigned* bar_gen, int* err, int poll) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   CholSmem& S = *reinterpret_cast<CholSmem*>(smem_raw);
-  const int tid = threadIdx.x;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const bool solver = warp == 2 || warp == 3;
   for (int k = 0; k < n; k += CNB) {
     const int nb = min(CNB, n - k);
-    // 1. the panel's diagonal block, factored by warp 0 (every CTA does the
-    //    same arithmetic, so all agree); identity-padded past n
+    const int base = k + nb;
+    const int lim = min(n, base + band);
+    const int nt = (lim - base + CNB - 1) / CNB;
+    const int ntiles = lim > base ? nt * (nt + 1) / 2 : 0;
+    // 1. diagonal block (identity-padded past n) and the first tile's panel rows
     for (int q = tid; q < CNB * CNB; q += blockDim.x) {
       const int i = q / CNB, j = q % CNB;
       S.W[i][j] = (i < nb && j < nb && j <= i) ? (i - j <= band ? ldcg(A + bidx(k + i, k + j, band, ldb)) : 0.0)
                                                : (i == j ? 1.0 : 0.0);
     }
+    double x[CNB];
+    if (solver && (int)blockIdx.x < ntiles) {
+      int ti, tj;
+      tile_of(blockIdx.x, ti, tj);
+      const int r0 = warp == 2 ? base + CNB * ti : base + CNB * tj;
+      panel_load(A, band, ldb, k, nb, r0 + lane, lim, x);
+    }
     __syncthreads();
-    if (tid < 32) {
-      const int lane = tid;
+    // 2. factor (every CTA does the same arithmetic, so all agree)
+    if (warp == 0) {
       double wr[CNB];
 #pragma unroll
       for (int t = 0; t < CNB; ++t) wr[t] = S.W[lane][t];
       bool bad = false;
-#pragma unroll
-      for (int j = 0; j < CNB; ++j) {
-        const double d = __shfl_sync(0xffffffffu, wr[j], j);
-        const bool ok = d > 0.0 && isfinite(d);
-        const double dd = ok ? d : 1.0;
-        const double rs = rsqrt(dd);
-        const double lj = wr[j];
-        if (lane == j) {
-          bad |= !ok;
-          S.Ld[j][j] = dd * rs;
-          S.invd[j] = rs;
-        } else {
-          S.Ld[lane][j] = lane > j ? lj * rs : 0.0;
-        }
-        const double w = lj * (rs * rs);
-#pragma unroll
-        for (int t = j + 1; t < CNB; ++t) {
-          const double ct = __shfl_sync(0xffffffffu, wr[j], t);
-          if (t <= lane) wr[t] -= ct * w;
-        }
-      }
+      chol_step<0>(wr, lane, S, bad);
       bad = __any_sync(0xffffffffu, bad);
       if (lane == 0) S.bad = bad ? 1 : 0;
     }
@@ -214,37 +232,18 @@ __global__ void __launch_bounds__(256) k_band_chol(int n, int band, long long ld
       }
       if (tid == 0 && S.bad) *flag = 1;
     }
-    // 2. trailing tiles of the band window: solve their panel rows, write
-    //    the factor rows (owner of the diagonal tile), update
-    const int base = k + nb;
-    const int lim = min(n, base + band);
-    const int nt = (lim - base + CNB - 1) / CNB;
-    const int ntiles = lim > base ? nt * (nt + 1) / 2 : 0;
+    // 3. trailing tiles of the band window
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
       int ti, tj;
       tile_of(t, ti, tj);
       const int i0 = base + CNB * ti, j0 = base + CNB * tj;
       if (i0 - (j0 + CNB - 1) > band) continue;  // whole tile outside the band (uniform)
-      panel_solve(A, band, ldb, k, nb, i0, lim, S, S.Pi);
-      if (tj != ti) {
-        __syncthreads();
-        if (tid >= 32 && tid < 64) {
-          // second row tile by warp 1 (same code path, shifted thread index)
-          const int tt = tid - 32;
-          const int i = j0 + tt;
-          double x[CNB];
+      if (warp == 2 || (warp == 3 && tj != ti)) {
+        if (t != (int)blockIdx.x) panel_load(A, band, ldb, k, nb, (warp == 2 ? i0 : j0) + lane, lim, x);
+        solve_step<0>(x, S);
+        double(*P)[CNB + 1] = warp == 2 ? S.Pi : S.Pj;
 #pragma unroll
-          for (int j = 0; j < CNB; ++j)
-            x[j] = (i < lim && j < nb && i - (k + j) <= band) ? ldcg(A + bidx(i, k + j, band, ldb)) : 0.0;
-#pragma unroll
-          for (int j = 0; j < CNB; ++j) {
-            x[j] *= S.invd[j];
-#pragma unroll
-            for (int q = j + 1; q < CNB; ++q) x[q] -= x[j] * S.Ld[q][j];
-          }
-#pragma unroll
-          for (int j = 0; j < CNB; ++j) S.Pj[tt][j] = x[j];
-        }
+        for (int j = 0; j < CNB; ++j) P[lane][j] = x[j];
       }
       __syncthreads();
       double(*Pj)[CNB + 1] = (tj == ti) ? S.Pi : S.Pj;
@@ -269,7 +268,10 @@ __global__ void __launch_bounds__(256) k_band_chol(int n, int band, long long ld
 #pragma unroll
         for (int m = 0; m < 4; ++m) {
           const int j = j0 + c0 + m;
-          if (j < lim && j <= i && i - j <= band) A[bidx(i, j, band, ldb)] -= acc[m];
+          if (j < lim && j <= i && i - j <= band) {
+            double* a = A + bidx(i, j, band, ldb);
+            *a = ldcg(a) - acc[m];
+          }
         }
       }
       __syncthreads();
@@ -278,253 +280,252 @@ __global__ void __launch_bounds__(256) k_band_chol(int n, int band, long long ld
   }
 }
 
-}  // namespace cst
-}  // namespace topo
+// ------------------------------------------------------ inverse of L
+// Dinv_I = L_II^-1 for every 32x32 diagonal block (identity past n): thread c
+// forms column c by forward substitution.
+__global__ void __launch_bounds__(CNB) k_diag_inverse(int n, int band, long long ldb, const double* __restrict__ L,
+                                                      double* __restrict__ Dinv) {
+  __shared__ double Ls[CNB][CNB + 1];
+  __shared__ double X[CNB][CNB + 1];
+  const int I = blockIdx.x, c = threadIdx.x;
+  const long long r0 = (long long)I * CNB;
+  for (int r = 0; r < CNB; ++r) {
+    const long long i = r0 + r;
+    Ls[r][c] = (i < n && c <= r && r - c <= band) ? L[bidx(i, r0 + c, band, ldb)] : (r == c ? 1.0 : 0.0);
+  }
+  __syncwarp();
+  for (int r = 0; r < CNB; ++r) {
+    double v = (r == c) ? 1.0 : 0.0;
+    for (int q = c; q < r; ++q) v -= Ls[r][q] * X[q][c];
+    X[r][c] = r >= c ? v / Ls[r][r] : 0.0;
+  }
+  __syncwarp();
+  for (int r = 0; r < CNB; ++r) Dinv[(long long)I * CNB * CNB + r * CNB + c] = X[r][c];
+}
 
-namespace topo {
-namespace cst {
-
-// ------------------------------------------------------ block inverses
-// Di_b = L_bb^-1 for every plane block: CTA (s, b) owns the 32 columns
-// [32s, 32s+32) of block b and walks its 32-row sub-blocks I >= s:
-//   R   = E - L[rows of I, cols 32s .. 32I) W[32s .. 32I, strip]
-//   W_I = L_II^-1 R  (forward substitution, one thread per column)
-// The strip's rows of W stay in shared memory (<= kMaxBlock rows).
-constexpr int kMaxBlock = 512;  // largest plane block (3 (NY+1)(NZ+1) free DoFs)
-struct InvSmem {
-  double Wst[kMaxBlock][CNB + 1];
-  double Lc[CNB][CNB + 1];
-  double R[CNB][CNB + 1];
+// W = L^-1 by forward substitution, one strip of TWC columns per CTA. Every
+// column of W is an independent forward substitution, so the strips need no
+// communication: CTA J owns columns [TWC J, TWC J + TWC) and walks the
+// 32-row blocks I from the one holding its first column to the last:
+//   R    = E - sum_{k in [max(j0, 32I-band), 32I)} L[32I.., k] W[k, strip]
+//   W_I  = Dinv_I R                    (E: the identity on these rows/columns)
+// Every W read is of rows this CTA wrote in an earlier step (visible after
+// __syncthreads). The strip of column 0 is the critical path, so strips are
+// narrower than a row block. A step reads its L rows from L2 (all strips at
+// block row I read the same rows) in 64-wide chunks, the next chunk
+// prefetched into registers. Warp w takes the chunk columns k = w, w+8, ...;
+// lane r keeps row r of the 32 x TWC partial product; the 8 warp partials are
+// summed through shared memory.
+// W goes to W64 (lower part, FP64) and to the apply matrix (C64 or C32) as W
+// in the lower triangle and W^T in the strict upper triangle, row stride ldc.
+constexpr int TIT = 256, TKC = 64, TWC = 16;
+struct TriSmem {
+  double Ls[CNB][TKC + 1];
+  double Wc[TKC][TWC];
+  double red[TIT / 32][CNB][TWC + 1];
+  double Rs[CNB][TWC + 1];
+  double Ds[CNB][CNB + 1];
 };
 
-__global__ void __launch_bounds__(256) k_block_inverse(const int* __restrict__ boff, int band, long long ldb,
-                                                       const double* __restrict__ L, const long long* __restrict__ dioff,
-                                                       double* __restrict__ DI) {
+__global__ void __launch_bounds__(TIT) k_tri_inverse(int n, int band, long long ldb, const double* __restrict__ L,
+                                                     const double* __restrict__ Dinv, double* W64, long long ldc,
+                                                     double* C64, float* C32) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  InvSmem& S = *reinterpret_cast<InvSmem*>(smem_raw);
-  const int b = blockIdx.y, s = blockIdx.x;
-  const int o = boff[b], m = boff[b + 1] - o;
-  const int c0 = CNB * s;
-  if (c0 >= m) return;
-  const int tid = threadIdx.x;
-  const int nsub = (m + CNB - 1) / CNB;
-  const int r = tid >> 3, cq = (tid & 7) * 4;
-  for (int I = s; I < nsub; ++I) {
-    const int i0 = CNB * I;
-    // R = E - L[i0.., c0..i0) W[c0..i0, :]
-    double acc[4] = {0.0, 0.0, 0.0, 0.0};
-    for (int k0 = c0; k0 < i0; k0 += CNB) {
+  TriSmem& S = *reinterpret_cast<TriSmem*>(smem_raw);
+  const int nT = (n + CNB - 1) / CNB;
+  const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+  const int j0 = blockIdx.x * TWC;
+  if (j0 >= n) return;  // uniform over the CTA
+  constexpr int PL = CNB * TKC / TIT;  // L values fetched per thread per chunk
+  constexpr int PW = TKC * TWC / TIT;  // W values fetched per thread per chunk
+  constexpr int PO = CNB * TWC / TIT;  // outputs per thread per step
+  static_assert(PL * TIT == CNB * TKC && PW * TIT == TKC * TWC && PO * TIT == CNB * TWC, "tile split");
+  double pl[PL], pw[PW];
+  for (int I = j0 / CNB; I < nT; ++I) {
+    const int i0 = I * CNB;
+    const int klo = max(j0, i0 - band);
+    auto fetch = [&](int k0) {
+#pragma unroll
+      for (int m = 0; m < PL; ++m) {
+        const int q = t + TIT * m;
+        const int i = i0 + q / TKC, k = k0 + q % TKC;
+        pl[m] = (i < n && k < i0 && i - k <= band) ? L[bidx(i, k, band, ldb)] : 0.0;
+      }
+#pragma unroll
+      for (int m = 0; m < PW; ++m) {
+        const int q = t + TIT * m;
+        const int kw = k0 + q / TWC, cw = j0 + q % TWC;
+        pw[m] = (kw < i0 && cw < n && cw <= kw) ? W64[(long long)kw * ldc + cw] : 0.0;
+      }
+    };
+    double acc[TWC];
+#pragma unroll
+    for (int c = 0; c < TWC; ++c) acc[c] = 0.0;
+    if (klo < i0) fetch(klo);
+    for (int k0 = klo; k0 < i0; k0 += TKC) {
       __syncthreads();
-      for (int q = tid; q < CNB * CNB; q += blockDim.x) {
-        const int rr = q / CNB, kk = q % CNB;
-        const long long gi = o + i0 + rr, gk = o + k0 + kk;
-        S.Lc[rr][kk] = (i0 + rr < m && k0 + kk < i0 && gi - gk <= band) ? L[bidx(gi, gk, band, ldb)] : 0.0;
+#pragma unroll
+      for (int m = 0; m < PL; ++m) {
+        const int q = t + TIT * m;
+        S.Ls[q / TKC][q % TKC] = pl[m];
+      }
+#pragma unroll
+      for (int m = 0; m < PW; ++m) {
+        const int q = t + TIT * m;
+        S.Wc[q / TWC][q % TWC] = pw[m];
       }
       __syncthreads();
-#pragma unroll 8
-      for (int kk = 0; kk < CNB; ++kk) {
-        const double l = S.Lc[r][kk];
-        if (k0 + kk < i0) {
+      if (k0 + TKC < i0) fetch(k0 + TKC);
+#pragma unroll 4
+      for (int m = 0; m < TKC / 8; ++m) {
+        const int kk = warp + 8 * m;
+        const double a = S.Ls[lane][kk];
+        const double2* wr = reinterpret_cast<const double2*>(&S.Wc[kk][0]);
 #pragma unroll
-          for (int q = 0; q < 4; ++q) acc[q] = fma(l, S.Wst[k0 + kk][cq + q], acc[q]);
+        for (int c2 = 0; c2 < TWC / 2; ++c2) {
+          const double2 w = wr[c2];
+          acc[2 * c2] = fma(a, w.x, acc[2 * c2]);
+          acc[2 * c2 + 1] = fma(a, w.y, acc[2 * c2 + 1]);
         }
       }
     }
+#pragma unroll
+    for (int c = 0; c < TWC; ++c) S.red[warp][lane][c] = acc[c];
+    for (int q = t; q < CNB * CNB; q += TIT) S.Ds[q >> 5][q & 31] = Dinv[(long long)I * CNB * CNB + q];
     __syncthreads();
 #pragma unroll
-    for (int q = 0; q < 4; ++q) S.R[r][cq + q] = ((i0 + r == c0 + cq + q) ? 1.0 : 0.0) - acc[q];
-    // the diagonal sub-block L_II
-    for (int q = tid; q < CNB * CNB; q += blockDim.x) {
-      const int rr = q / CNB, kk = q % CNB;
-      S.Lc[rr][kk] = (i0 + rr < m && i0 + kk < m && kk <= rr)
-                         ? (rr - kk <= band ? L[bidx(o + i0 + rr, o + i0 + kk, band, ldb)] : 0.0)
-                         : (rr == kk ? 1.0 : 0.0);
+    for (int p = 0; p < PO; ++p) {
+      const int q = t + TIT * p;
+      const int r = q / TWC, c = q % TWC;
+      double v = (i0 + r == j0 + c) ? 1.0 : 0.0;
+#pragma unroll
+      for (int w = 0; w < TIT / 32; ++w) v -= S.red[w][r][c];
+      S.Rs[r][c] = v;
     }
     __syncthreads();
-    if (tid < CNB) {
-      const int c = tid;
-      for (int rr = 0; rr < CNB; ++rr) {
-        double v = S.R[rr][c];
-        for (int q = 0; q < rr; ++q) v -= S.Lc[rr][q] * S.Wst[i0 + q][c];
-        S.Wst[i0 + rr][c] = (i0 + rr < m) ? v / S.Lc[rr][rr] : 0.0;
+    double wv[PO];
+#pragma unroll
+    for (int p = 0; p < PO; ++p) {
+      const int q = t + TIT * p;
+      const int r = q / TWC, c = q % TWC;
+      double v = 0.0;
+      for (int m = 0; m <= r; ++m) v = fma(S.Ds[r][m], S.Rs[m][c], v);
+      wv[p] = v;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int p = 0; p < PO; ++p) {
+      const int q = t + TIT * p;
+      const int r = q / TWC, c = q % TWC;
+      const int i = i0 + r, col = j0 + c;
+      S.Rs[r][c] = wv[p];
+      if (i < n && col < n && col <= i) {
+        W64[(long long)i * ldc + col] = wv[p];
+        if (C64 != nullptr && C64 != W64) C64[(long long)i * ldc + col] = wv[p];
+        if (C32 != nullptr) C32[(long long)i * ldc + col] = (float)wv[p];
+      }
+    }
+    __syncthreads();
+    // transposed copy: rows j0 .. j0+TWC-1 of the upper triangle, columns i0 .. i0+31
+    for (int q = t; q < TWC * CNB; q += TIT) {
+      const int cr = j0 + q / CNB, ic = i0 + q % CNB;
+      if (cr < n && ic < n && ic > cr) {
+        const double v = S.Rs[q % CNB][q / CNB];
+        if (C64 != nullptr) C64[(long long)cr * ldc + ic] = v;
+        if (C32 != nullptr) C32[(long long)cr * ldc + ic] = (float)v;
       }
     }
     __syncthreads();
   }
-  // write the strip: rows c0.. m-1 (entries above the diagonal are zero)
-  double* D = DI + dioff[b];
-  for (int q = tid; q < (m - c0) * CNB; q += blockDim.x) {
-    const int rr = c0 + q / CNB, c = c0 + q % CNB;
-    if (c < m) D[(long long)rr * m + c] = (c <= rr) ? S.Wst[rr][c - c0] : 0.0;
-  }
-  // and the zero upper part of these columns
-  for (int q = tid; q < c0 * CNB; q += blockDim.x) {
-    const int rr = q / CNB, c = c0 + q % CNB;
-    if (c < m) D[(long long)rr * m + c] = 0.0;
-  }
-}
-
-// L_{b,b-1} (dense, rows of block b x columns of block b-1) from band storage.
-__global__ void k_extract_sub(const int* __restrict__ boff, int band, long long ldb, const double* __restrict__ L,
-                              const long long* __restrict__ soff, double* __restrict__ Ls) {
-  const int b = blockIdx.y + 1;
-  const int o = boff[b], m = boff[b + 1] - o, op = boff[b - 1], mp = o - op;
-  double* D = Ls + soff[b];
-  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < (long long)m * mp;
-       q += (long long)gridDim.x * blockDim.x) {
-    const long long i = o + q / mp, j = op + q % mp;
-    D[q] = (i - j <= band) ? L[bidx(i, j, band, ldb)] : 0.0;
-  }
-}
-
-// Batched C_b = op(A_b) op(B_b) in FP64 with strided operands:
-// A(i,k) = A[i*sai + k*sak], B(k,j) = B[k*sbk + j*sbj]; C row-major (m x n).
-struct GemmJob {
-  const double* A;
-  const double* B;
-  void* C;
-  int m, n, kdim;
-  int sai, sak, sbk, sbj;
-};
-
-template <typename TO>
-__global__ void __launch_bounds__(256) k_gemm_batched(const GemmJob* __restrict__ jobs) {
-  const GemmJob jb = jobs[blockIdx.z];
-  const int i0 = blockIdx.y * 32, j0 = blockIdx.x * 32;
-  if (i0 >= jb.m || j0 >= jb.n) return;
-  __shared__ double As[32][33], Bs[32][33];
-  const int tid = threadIdx.x, r = tid >> 3, cq = (tid & 7) * 4;
-  double acc[4] = {0.0, 0.0, 0.0, 0.0};
-  for (int k0 = 0; k0 < jb.kdim; k0 += 32) {
-    __syncthreads();
-    for (int q = tid; q < 1024; q += 256) {
-      const int a = q / 32, bq = q % 32;
-      As[a][bq] = (i0 + a < jb.m && k0 + bq < jb.kdim) ? jb.A[(long long)(i0 + a) * jb.sai + (long long)(k0 + bq) * jb.sak] : 0.0;
-      Bs[a][bq] = (k0 + a < jb.kdim && j0 + bq < jb.n) ? jb.B[(long long)(k0 + a) * jb.sbk + (long long)(j0 + bq) * jb.sbj] : 0.0;
-    }
-    __syncthreads();
-#pragma unroll 8
-    for (int kk = 0; kk < 32; ++kk) {
-      const double a = As[r][kk];
-#pragma unroll
-      for (int q = 0; q < 4; ++q) acc[q] = fma(a, Bs[kk][cq + q], acc[q]);
-    }
-  }
-  TO* C = reinterpret_cast<TO*>(jb.C);
-  if (i0 + r < jb.m) {
-#pragma unroll
-    for (int q = 0; q < 4; ++q)
-      if (j0 + cq + q < jb.n) C[(long long)(i0 + r) * jb.n + j0 + cq + q] = (TO)acc[q];
-  }
-}
-
-template <typename TO>
-__global__ void k_convert_copy(long long n, const double* __restrict__ src, TO* __restrict__ dst) {
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-    dst[i] = (TO)src[i];
 }
 
 // --------------------------------------------------------------- apply
-// One cluster of CL CTAs; block offsets, sizes and matrix offsets in a small
-// device table. y (forward) and z (backward) live in global memory (L2),
-// read with .cg loads after each cluster barrier (release/acquire at
-// cluster scope orders the writes of every CTA of the cluster).
-constexpr int CL = 8;
-constexpr int AT = 256;
-
-struct ApplyPlan {
-  int nb;
-  long long nfull;       // length of the full vectors rhs and x
-  const int* boff;       // nb+1
-  const int* link;       // link[b] = 1: block b couples to b-1
-  const long long* dioff;  // Di_b, m_b x m_b
-  const long long* moff;   // M_b, m_b x m_{b-1}
-  const long long* noff;   // N_b, m_b x m_{b+1}
-};
-
-__device__ __forceinline__ void cluster_sync() {
-  asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+// z = W^T (W r) over C (W below and on the diagonal, W^T above): pass one
+// y = W r_c (row i reads C[i][0..i]), pass two z_c = W^T y (row j reads
+// C[j][j..n-1]). One warp per row, 16-byte loads (ldc is a multiple of 32
+// elements, so every row starts 16-byte aligned), two loads in flight per
+// lane, FP64 accumulation. The compact right-hand side is gathered once; both
+// passes read the compact vectors (n doubles) through L1.
+template <typename T>
+__global__ void k_coarse_gather(int n, long long nfull, const int* __restrict__ free_list, const T* __restrict__ rhs,
+                                double* __restrict__ rc, const KrylovState* st) {
+  if (st != nullptr && st->done) return;
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j < n) {
+    const int f = free_list[j];
+    rc[j] = topo_in_range(f, nfull) ? (double)rhs[f] : 0.0;
+  }
 }
-__device__ __forceinline__ unsigned cluster_rank() {
-  unsigned r;
-  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
-  return r;
+
+template <typename TX>
+__global__ void __launch_bounds__(256) k_coarse_lower(int n, long long ldc, const TX* __restrict__ C,
+                                                      const double* __restrict__ rc, double* __restrict__ y,
+                                                      const KrylovState* st) {
+  if (st != nullptr && st->done) return;
+  const int row = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+  if (row >= n) return;
+  constexpr int V = 16 / sizeof(TX);
+  const TX* Ci = C + (long long)row * ldc;
+  double acc = 0.0;
+  int j = lane * V;
+  for (; j + 32 * V <= row; j += 64 * V) {  // two 16-byte loads in flight
+    TX v[V], w[V];
+    *reinterpret_cast<uint4*>(v) = __ldg(reinterpret_cast<const uint4*>(Ci + j));
+    const bool two = j + 32 * V <= row;
+    if (two) *reinterpret_cast<uint4*>(w) = __ldg(reinterpret_cast<const uint4*>(Ci + j + 32 * V));
+#pragma unroll
+    for (int q = 0; q < V; ++q) acc += (double)v[q] * __ldg(rc + j + q);
+    if (two) {
+#pragma unroll
+      for (int q = 0; q < V; ++q)
+        if (j + 32 * V + q <= row) acc += (double)w[q] * __ldg(rc + j + 32 * V + q);
+    }
+  }
+  for (; j <= row; j += 32 * V) {
+    TX v[V];
+    *reinterpret_cast<uint4*>(v) = __ldg(reinterpret_cast<const uint4*>(Ci + j));
+#pragma unroll
+    for (int q = 0; q < V; ++q)
+      if (j + q <= row) acc += (double)v[q] * __ldg(rc + j + q);
+  }
+  acc = warp_sum(acc);
+  if (lane == 0) y[row] = acc;
 }
 
 template <typename T, typename TX>
-__global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(AT)
-    k_coarsest_apply(int n, ApplyPlan P, const TX* __restrict__ DI, const TX* __restrict__ M, const TX* __restrict__ N,
-                     const int* __restrict__ free_list, const T* __restrict__ rhs, double* __restrict__ y,
-                     double* __restrict__ z, T* __restrict__ x, const KrylovState* st) {
+__global__ void __launch_bounds__(256) k_coarse_upper(int n, long long nfull, long long ldc, const TX* __restrict__ C,
+                                                      const int* __restrict__ free_list,
+                                                      const double* __restrict__ y, T* __restrict__ x,
+                                                      const KrylovState* st) {
   if (st != nullptr && st->done) return;
-  __shared__ double vb[kMaxBlock];
-  const int rank = (int)cluster_rank();
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int gw = rank * (AT / 32) + warp, nw = CL * (AT / 32);
-  // 1. y_b = Di_b r_b for every block (one warp per row)
-  for (int b = 0; b < P.nb; ++b) {
-    const int o = P.boff[b], m = P.boff[b + 1] - o;
-    const TX* D = DI + P.dioff[b];
-    for (int i = gw; i < m; i += nw) {
-      double acc = 0.0;
-      for (int j = lane; j <= i; j += 32) {
-        const int f = free_list[o + j];
-        if (topo_in_range(f, P.nfull)) acc += (double)D[(long long)i * m + j] * (double)rhs[f];
-      }
-      acc = warp_sum(acc);
-      if (lane == 0) y[o + i] = acc;
-    }
+  const int row = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+  if (row >= n) return;
+  constexpr int V = 16 / sizeof(TX);
+  const TX* Cj = C + (long long)row * ldc;
+  double acc = 0.0;
+  int i = (row / V) * V + lane * V;
+  for (; i + 32 * V < n; i += 64 * V) {  // two 16-byte loads in flight
+    TX v[V], w[V];
+    *reinterpret_cast<uint4*>(v) = __ldg(reinterpret_cast<const uint4*>(Cj + i));
+    *reinterpret_cast<uint4*>(w) = __ldg(reinterpret_cast<const uint4*>(Cj + i + 32 * V));
+#pragma unroll
+    for (int q = 0; q < V; ++q)
+      if (i + q >= row) acc += (double)v[q] * __ldg(y + i + q);
+#pragma unroll
+    for (int q = 0; q < V; ++q)
+      if (i + 32 * V + q < n) acc += (double)w[q] * __ldg(y + i + 32 * V + q);
   }
-  cluster_sync();
-  // 2. forward sweep: y_b -= M_b y_{b-1}
-  for (int b = 1; b < P.nb; ++b) {
-    const int o = P.boff[b], m = P.boff[b + 1] - o, op = P.boff[b - 1], mp = o - op;
-    if (P.link[b]) {
-      for (int j = threadIdx.x; j < mp; j += AT) vb[j] = __ldcg(y + op + j);
-      __syncthreads();
-      const TX* Mb = M + P.moff[b];
-      for (int i = gw; i < m; i += nw) {
-        double acc = 0.0;
-        for (int j = lane; j < mp; j += 32) acc += (double)Mb[(long long)i * mp + j] * vb[j];
-        acc = warp_sum(acc);
-        if (lane == 0) y[o + i] = __ldcg(y + o + i) - acc;
-      }
-      __syncthreads();
-    }
-    cluster_sync();
+  for (; i < n; i += 32 * V) {
+    TX v[V];
+    *reinterpret_cast<uint4*>(v) = __ldg(reinterpret_cast<const uint4*>(Cj + i));
+#pragma unroll
+    for (int q = 0; q < V; ++q)
+      if (i + q >= row && i + q < n) acc += (double)v[q] * __ldg(y + i + q);
   }
-  // 3. z_b = Di_b^T y_b (one thread per column)
-  for (int b = 0; b < P.nb; ++b) {
-    const int o = P.boff[b], m = P.boff[b + 1] - o;
-    const TX* D = DI + P.dioff[b];
-    for (int j = rank * AT + threadIdx.x; j < m; j += CL * AT) {
-      double acc = 0.0;
-      for (int i = j; i < m; ++i) acc += (double)D[(long long)i * m + j] * __ldcg(y + o + i);
-      z[o + j] = acc;
-    }
-  }
-  cluster_sync();
-  // 4. backward sweep: z_b -= N_b z_{b+1}
-  for (int b = P.nb - 2; b >= 0; --b) {
-    const int o = P.boff[b], m = P.boff[b + 1] - o, on = P.boff[b + 1], mn = P.boff[b + 2] - on;
-    if (P.link[b + 1]) {
-      for (int j = threadIdx.x; j < mn; j += AT) vb[j] = __ldcg(z + on + j);
-      __syncthreads();
-      const TX* Nb = N + P.noff[b];
-      for (int i = gw; i < m; i += nw) {
-        double acc = 0.0;
-        for (int j = lane; j < mn; j += 32) acc += (double)Nb[(long long)i * mn + j] * vb[j];
-        acc = warp_sum(acc);
-        if (lane == 0) z[o + i] = __ldcg(z + o + i) - acc;
-      }
-      __syncthreads();
-    }
-    cluster_sync();
-  }
-  // 5. scatter
-  for (int i = rank * AT + threadIdx.x; i < n; i += CL * AT) {
-    const int f = free_list[i];
-    if (topo_in_range(f, P.nfull)) x[f] = (T)__ldcg(z + i);
+  acc = warp_sum(acc);
+  if (lane == 0) {
+    const int f = free_list[row];
+    if (topo_in_range(f, nfull)) x[f] = (T)acc;
   }
 }
 
@@ -535,45 +536,9 @@ CoarsestPlan coarsest_plan(const Grid& g, const std::vector<int>& free_list) {
   CoarsestPlan p;
   p.n = (int)free_list.size();
   p.nfull = g.ndof;
-  // plane of a compact DoF: node = dof/3, plane = node / (NY*NZ)
-  const long long plane_nodes = (long long)g.NY * g.NZ;
-  std::vector<int> plane_of(p.n);
-  for (int i = 0; i < p.n; ++i) plane_of[i] = (int)((free_list[i] / 3) / plane_nodes);
-  p.boff.push_back(0);
-  p.link.push_back(0);
-  for (int i = 1; i <= p.n; ++i) {
-    if (i == p.n || plane_of[i] != plane_of[i - 1]) {
-      p.boff.push_back(i);
-      if (i < p.n) p.link.push_back(plane_of[i] == plane_of[i - 1] + 1 ? 1 : 0);
-    }
-  }
-  p.nb = (int)p.boff.size() - 1;
-  p.mmax = 0;
-  long long di = 0, ms = 0, ns = 0;
-  p.dioff.assign(p.nb, 0);
-  p.moff.assign(p.nb, 0);
-  p.noff.assign(p.nb, 0);
-  for (int b = 0; b < p.nb; ++b) {
-    const int m = p.boff[b + 1] - p.boff[b];
-    p.mmax = std::max(p.mmax, m);
-    p.dioff[b] = di;
-    di += (long long)m * m;
-    if (b > 0) {
-      p.moff[b] = ms;
-      ms += (long long)m * (p.boff[b] - p.boff[b - 1]);
-    }
-    if (b + 1 < p.nb) {
-      p.noff[b] = ns;
-      ns += (long long)m * (p.boff[b + 2] - p.boff[b + 1]);
-    }
-  }
-  p.di_size = di;
-  p.m_size = ms;
-  p.n_size = ns;
+  p.nt = (p.n + cst::CNB - 1) / cst::CNB;
   return p;
 }
-
-bool coarsest_supported(const CoarsestPlan& p) { return p.mmax <= cst::kMaxBlock; }
 
 void coarsest_alloc(CoarsestFactor& f, const CoarsestPlan& p, int band, bool f64, void* (*alloc_bytes)(void*, size_t),
                     void* ctx) {
@@ -581,68 +546,17 @@ void coarsest_alloc(CoarsestFactor& f, const CoarsestPlan& p, int band, bool f64
   f.band = band;
   f.ldb = band + 1;
   f.f64 = f64;
-  const size_t nb = (size_t)std::max(p.n, 1) * f.ldb;
-  f.A = (double*)A(nb * sizeof(double));
-  f.L = (double*)A(nb * sizeof(double));
-  f.DI64 = (double*)A(std::max<long long>(p.di_size, 1) * sizeof(double));
-  f.LS64 = (double*)A(std::max<long long>(p.m_size, 1) * sizeof(double));
-  const size_t es = f64 ? sizeof(double) : sizeof(float);
-  f.DI = A(std::max<long long>(p.di_size, 1) * es);
-  f.M = A(std::max<long long>(p.m_size, 1) * es);
-  f.N = A(std::max<long long>(p.n_size, 1) * es);
+  const int n = std::max(p.n, 1);
+  const size_t nbs = (size_t)n * f.ldb;
+  f.A = (double*)A(nbs * sizeof(double));
+  f.L = (double*)A(nbs * sizeof(double));
+  f.Dinv = (double*)A((size_t)std::max(p.nt, 1) * cst::CNB * cst::CNB * sizeof(double));
+  f.ldc = ((long long)n + 31) / 32 * 32;
+  f.W64 = (double*)A((size_t)n * f.ldc * sizeof(double));
+  f.C = f64 ? (void*)f.W64 : A((size_t)n * f.ldc * sizeof(float));
   f.flag = (int*)A(sizeof(int) * 4);
   f.bar = (unsigned*)A(sizeof(unsigned) * 4);
   f.err = f.flag + 1;
-  // device copies of the plan
-  f.d_boff = (int*)A(sizeof(int) * (p.nb + 1));
-  f.d_link = (int*)A(sizeof(int) * std::max(p.nb, 1));
-  f.d_dioff = (long long*)A(sizeof(long long) * std::max(p.nb, 1));
-  f.d_moff = (long long*)A(sizeof(long long) * std::max(p.nb, 1));
-  f.d_noff = (long long*)A(sizeof(long long) * std::max(p.nb, 1));
-  f.d_jobs = A(sizeof(cst::GemmJob) * 2 * std::max(p.nb, 1));
-  TOPO_CUDA_CHECK(cudaMemcpy(f.d_boff, p.boff.data(), sizeof(int) * (p.nb + 1), cudaMemcpyHostToDevice));
-  TOPO_CUDA_CHECK(cudaMemcpy(f.d_link, p.link.data(), sizeof(int) * p.nb, cudaMemcpyHostToDevice));
-  TOPO_CUDA_CHECK(cudaMemcpy(f.d_dioff, p.dioff.data(), sizeof(long long) * p.nb, cudaMemcpyHostToDevice));
-  TOPO_CUDA_CHECK(cudaMemcpy(f.d_moff, p.moff.data(), sizeof(long long) * p.nb, cudaMemcpyHostToDevice));
-  TOPO_CUDA_CHECK(cudaMemcpy(f.d_noff, p.noff.data(), sizeof(long long) * p.nb, cudaMemcpyHostToDevice));
-  // GEMM jobs: M_b = Di_b L_{b,b-1} (b >= 1, linked), N_b = Di_b^T L_{b+1,b}^T
-  std::vector<cst::GemmJob> jobs;
-  for (int b = 0; b < p.nb; ++b) {
-    const int m = p.boff[b + 1] - p.boff[b];
-    if (b >= 1 && p.link[b]) {
-      const int mp = p.boff[b] - p.boff[b - 1];
-      cst::GemmJob j{};
-      j.A = f.DI64 + p.dioff[b];
-      j.B = f.LS64 + p.moff[b];
-      j.C = (char*)f.M + p.moff[b] * es;
-      j.m = m;
-      j.n = mp;
-      j.kdim = m;
-      j.sai = m;
-      j.sak = 1;
-      j.sbk = mp;
-      j.sbj = 1;
-      jobs.push_back(j);
-    }
-    if (b + 1 < p.nb && p.link[b + 1]) {
-      const int mn = p.boff[b + 2] - p.boff[b + 1];
-      cst::GemmJob j{};
-      j.A = f.DI64 + p.dioff[b];  // Di_b^T: A(i,k) = Di[k][i]
-      j.B = f.LS64 + p.moff[b + 1];  // L_{b+1,b} is mn x m; its transpose: B(k,j) = L[j][k]
-      j.C = (char*)f.N + p.noff[b] * es;
-      j.m = m;
-      j.n = mn;
-      j.kdim = m;
-      j.sai = 1;
-      j.sak = m;
-      j.sbk = 1;
-      j.sbj = m;
-      jobs.push_back(j);
-    }
-  }
-  f.njobs = (int)jobs.size();
-  if (!jobs.empty())
-    TOPO_CUDA_CHECK(cudaMemcpy(f.d_jobs, jobs.data(), sizeof(cst::GemmJob) * jobs.size(), cudaMemcpyHostToDevice));
   // persistent factorisation: cooperative grid sized by co-residency
   int dev = 0, nsm = 0, per_sm = 0;
   TOPO_CUDA_CHECK(cudaGetDevice(&dev));
@@ -652,8 +566,8 @@ void coarsest_alloc(CoarsestFactor& f, const CoarsestPlan& p, int band, bool f64
   TOPO_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cst::k_band_chol, 256, sizeof(cst::CholSmem)));
   const int tiles_max = ((band + cst::CNB - 1) / cst::CNB) * ((band + cst::CNB - 1) / cst::CNB + 1) / 2;
   f.chol_grid = std::max(1, std::min(std::min(nsm * std::max(per_sm, 1), nsm), std::max(tiles_max, 1)));
-  TOPO_CUDA_CHECK(cudaFuncSetAttribute(cst::k_block_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)sizeof(cst::InvSmem)));
+  TOPO_CUDA_CHECK(cudaFuncSetAttribute(cst::k_tri_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)sizeof(cst::TriSmem)));
   f.plan = p;
 }
 
@@ -698,26 +612,11 @@ void coarsest_factor(CoarsestFactor& f, cudaStream_t s) {
                                                 sizeof(cst::CholSmem), s));
     count_launches(1);
   }
-  const int strips = (p.mmax + cst::CNB - 1) / cst::CNB;
-  cst::k_block_inverse<<<dim3(strips, p.nb), 256, sizeof(cst::InvSmem), s>>>(f.d_boff, f.band, f.ldb, f.L, f.d_dioff,
-                                                                              f.DI64);
+  cst::k_diag_inverse<<<p.nt, cst::CNB, 0, s>>>(n, f.band, f.ldb, f.L, f.Dinv);
   TOPO_LAUNCH_CHECK();
-  if (p.nb > 1) {
-    cst::k_extract_sub<<<dim3(64, p.nb - 1), 256, 0, s>>>(f.d_boff, f.band, f.ldb, f.L, f.d_moff, f.LS64);
-    TOPO_LAUNCH_CHECK();
-  }
-  if (f.njobs > 0) {
-    const int t = (p.mmax + 31) / 32;
-    if (f.f64) cst::k_gemm_batched<double><<<dim3(t, t, f.njobs), 256, 0, s>>>((const cst::GemmJob*)f.d_jobs);
-    else cst::k_gemm_batched<float><<<dim3(t, t, f.njobs), 256, 0, s>>>((const cst::GemmJob*)f.d_jobs);
-    TOPO_LAUNCH_CHECK();
-  }
-  if (f.f64) {
-    TOPO_CUDA_CHECK(cudaMemcpyAsync(f.DI, f.DI64, sizeof(double) * p.di_size, cudaMemcpyDeviceToDevice, s));
-  } else {
-    cst::k_convert_copy<float><<<1024, 256, 0, s>>>(p.di_size, f.DI64, (float*)f.DI);
-    TOPO_LAUNCH_CHECK();
-  }
+  cst::k_tri_inverse<<<(n + cst::TWC - 1) / cst::TWC, cst::TIT, sizeof(cst::TriSmem), s>>>(
+      n, f.band, f.ldb, f.L, f.Dinv, f.W64, f.ldc, f.f64 ? f.W64 : nullptr, f.f64 ? nullptr : (float*)f.C);
+  TOPO_LAUNCH_CHECK();
 }
 
 // Returns the non-positive-pivot flag (1) or a barrier timeout (< 0).
@@ -729,28 +628,39 @@ int coarsest_status(CoarsestFactor& f, cudaStream_t s) {
   return h[0] ? 1 : 0;
 }
 
+// work: 2n doubles (y, then the compact right-hand side).
 void coarsest_apply(const CoarsestFactor& f, bool vec64, const void* rhs, double* work, void* x, const KrylovState* st,
                     cudaStream_t s) {
   const CoarsestPlan& p = f.plan;
-  if (p.n == 0) return;
-  cst::ApplyPlan ap;
-  ap.nb = p.nb;
-  ap.nfull = p.nfull;
-  ap.boff = f.d_boff;
-  ap.link = f.d_link;
-  ap.dioff = f.d_dioff;
-  ap.moff = f.d_moff;
-  ap.noff = f.d_noff;
+  const int n = p.n;
+  if (n == 0) return;
+  const int wpb = 8;
+  const unsigned nb = (unsigned)((n + wpb - 1) / wpb);
+  const unsigned ng = (unsigned)((n + 255) / 256);
   double* y = work;
-  double* z = work + p.n;
+  double* rc = work + n;
   if (vec64) {
-    cst::k_coarsest_apply<double, double><<<cst::CL, cst::AT, 0, s>>>(p.n, ap, (const double*)f.DI, (const double*)f.M,
-                                                                      (const double*)f.N, f.d_free, (const double*)rhs,
-                                                                      y, z, (double*)x, st);
+    if (!f.f64) throw std::runtime_error("coarsest apply: FP64 vectors need the FP64 inverse");
+    cst::k_coarse_gather<double><<<ng, 256, 0, s>>>(n, p.nfull, f.d_free, (const double*)rhs, rc, st);
+    TOPO_LAUNCH_CHECK();
+    cst::k_coarse_lower<double><<<nb, 32 * wpb, 0, s>>>(n, f.ldc, (const double*)f.C, rc, y, st);
+    TOPO_LAUNCH_CHECK();
+    cst::k_coarse_upper<double, double><<<nb, 32 * wpb, 0, s>>>(n, p.nfull, f.ldc, (const double*)f.C, f.d_free, y,
+                                                                (double*)x, st);
   } else {
-    cst::k_coarsest_apply<float, float><<<cst::CL, cst::AT, 0, s>>>(p.n, ap, (const float*)f.DI, (const float*)f.M,
-                                                                    (const float*)f.N, f.d_free, (const float*)rhs, y, z,
-                                                                    (float*)x, st);
+    cst::k_coarse_gather<float><<<ng, 256, 0, s>>>(n, p.nfull, f.d_free, (const float*)rhs, rc, st);
+    TOPO_LAUNCH_CHECK();
+    if (f.f64) {
+      cst::k_coarse_lower<double><<<nb, 32 * wpb, 0, s>>>(n, f.ldc, (const double*)f.C, rc, y, st);
+      TOPO_LAUNCH_CHECK();
+      cst::k_coarse_upper<float, double><<<nb, 32 * wpb, 0, s>>>(n, p.nfull, f.ldc, (const double*)f.C, f.d_free, y,
+                                                                 (float*)x, st);
+    } else {
+      cst::k_coarse_lower<float><<<nb, 32 * wpb, 0, s>>>(n, f.ldc, (const float*)f.C, rc, y, st);
+      TOPO_LAUNCH_CHECK();
+      cst::k_coarse_upper<float, float><<<nb, 32 * wpb, 0, s>>>(n, p.nfull, f.ldc, (const float*)f.C, f.d_free, y,
+                                                                (float*)x, st);
+    }
   }
   TOPO_LAUNCH_CHECK();
 }

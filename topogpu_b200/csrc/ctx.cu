@@ -648,8 +648,8 @@ std::vector<double> pcg_graph_key(const topo_ctx* c) {
   std::vector<double> k = {(double)c->cheb_form, c->lam_safety, c->cheb_lower, (double)c->use_tc,
                            (double)c->cycle_gamma,
                            (double)c->fine_degree, (double)c->coarse_degree,
-                           (double)reinterpret_cast<uintptr_t>(c->C.cur.f.DI), (double)reinterpret_cast<uintptr_t>(c->C.cur.f.M),
-                           (double)reinterpret_cast<uintptr_t>(c->C.y), (double)c->C.n, (double)c->C.cur.f.plan.nb};
+                           (double)reinterpret_cast<uintptr_t>(c->C.cur.f.C), (double)reinterpret_cast<uintptr_t>(c->C.cur.f.W64),
+                           (double)reinterpret_cast<uintptr_t>(c->C.y), (double)c->C.n, (double)c->C.cur.f.plan.nt};
   for (const Level& Lv : c->L) {
     k.push_back(std::isnan(Lv.lam) ? -1.0 : Lv.lam);  // NaN (no estimate) would never compare equal
     k.push_back((double)Lv.degree);
@@ -1287,10 +1287,7 @@ int topo_set_problem(topo_ctx* c, const uint8_t* free_mask, const double* F, voi
       coarse_wait_background(c);
       c->C.have = false;
       CoarsestPlan plan = coarsest_plan(Lc.g, fl);
-      if (!coarsest_supported(plan))
-        throw std::runtime_error("coarsest level has an x-plane with " + std::to_string(plan.mmax) +
-                                 " free DoFs, above the 512 the direct solve supports; use more levels");
-      if (c->C.n != n || c->C.band != band || c->C.cur.S64c == nullptr || plan.boff != c->C.plan.boff) {
+      if (c->C.n != n || c->C.band != band || c->C.cur.S64c == nullptr) {
         c->C.n = n;
         c->C.band = band;
         c->C.plan = plan;

@@ -251,32 +251,28 @@ void prolong_add(bool vec64, const Grid& fine, const Grid& coarse, const void* e
 // coarsest level (coarsest.cu): band Cholesky of the free-DoF operator and
 // block sweeps over its x-plane blocks. Compact DoF i -> full DoF free[i].
 struct CoarsestPlan {
-  int n = 0, nb = 0, mmax = 0;
+  int n = 0;                                // free DoFs (compact rows)
+  int nt = 0;                               // 32-row blocks
   long long nfull = 0;                      // DoFs of the full coarsest-level vectors
-  std::vector<int> boff, link;              // block b = compact rows [boff[b], boff[b+1]); link[b]: couples to b-1
-  std::vector<long long> dioff, moff, noff; // offsets of Di_b, M_b (and L_{b,b-1}), N_b
-  long long di_size = 0, m_size = 0, n_size = 0;
 };
 struct CoarsestFactor {
   CoarsestPlan plan;
   int band = 0;
   long long ldb = 0;
-  bool f64 = true;                          // apply matrices and vectors in FP64 (else FP32)
+  bool f64 = true;                          // apply matrix and vectors in FP64 (else FP32)
   double *A = nullptr, *L = nullptr;        // band storage (n x (band+1)): operator, factor
-  double *DI64 = nullptr, *LS64 = nullptr;  // Di_b and L_{b,b-1} in FP64
-  void *DI = nullptr, *M = nullptr, *N = nullptr;  // apply matrices
+  double* Dinv = nullptr;                   // inverses of the 32x32 diagonal blocks of L
+  double* W64 = nullptr;                    // W = L^-1 (lower triangle, row stride ldc)
+  void* C = nullptr;                        // apply matrix: W below, W^T above (W64 itself in FP64)
+  long long ldc = 0;
   int* flag = nullptr;                      // [0] non-positive pivot, [1] barrier timeout
   int* err = nullptr;
   unsigned* bar = nullptr;
-  int *d_boff = nullptr, *d_link = nullptr;
-  long long *d_dioff = nullptr, *d_moff = nullptr, *d_noff = nullptr;
-  void* d_jobs = nullptr;
-  int njobs = 0, chol_grid = 1;
+  int chol_grid = 1;
   const int* d_free = nullptr;
   int kind = 0;                             // 0 none, 1 Cholesky, 2 Cholesky of K + eps I
 };
 CoarsestPlan coarsest_plan(const Grid& g, const std::vector<int>& free_list);
-bool coarsest_supported(const CoarsestPlan& p);
 void coarsest_alloc(CoarsestFactor& f, const CoarsestPlan& p, int band, bool f64, void* (*alloc_bytes)(void*, size_t),
                     void* ctx);
 void coarsest_assemble(CoarsestFactor& f, const Grid& g, const double* S, const int* dof_index, cudaStream_t s);
