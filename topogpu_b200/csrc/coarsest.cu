@@ -87,30 +87,25 @@ __device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
   return v;
 }
 
-// Sense-counting barrier over all CTAs of a cooperative launch. Thread 0
-// reads the generation, arrives, and the last arrival resets the count and
-// bumps the generation; the others poll it with a bound (a timeout raises
+// Grid barrier over all CTAs of a cooperative launch on a monotonic counter:
+// barrier number `epoch` (1, 2, ...) is passed once the counter reaches
+// epoch * nblocks. Thread 0 arrives and polls with a bound (a timeout raises
 // err and is reported to every thread of the CTA).
-__device__ bool grid_barrier(unsigned* count, unsigned* gen, unsigned nblocks, int* err, int poll) {
+__device__ bool grid_barrier(unsigned* count, unsigned epoch, unsigned nblocks, int* err, int poll) {
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
     int ok = 1;
-    const unsigned g0 = ld_acquire(gen);
     __threadfence();
-    if (atomicAdd(count, 1u) == nblocks - 1) {
-      atomicExch(count, 0u);
-      __threadfence();
-      atomicAdd(gen, 1u);
-    } else {
+    const unsigned target = epoch * nblocks;
+    if (atomicAdd(count, 1u) + 1u < target) {
       int it = 0;
-      while (ld_acquire(gen) == g0) {
+      while (ld_acquire(count) < target) {
         if (++it > poll) {
           ok = 0;
           atomicExch(err, 1);
           break;
         }
-        __nanosleep(40);
       }
     }
     __threadfence();
@@ -128,6 +123,7 @@ struct CholSmem {
   double W[CNB][CNB + 1];
   double Ld[CNB][CNB + 1];
   double invd[CNB];
+  double col[CNB];
   double Pi[CNB][CNB + 1];
   double Pj[CNB][CNB + 1];
   int bad;
@@ -142,10 +138,14 @@ __device__ __forceinline__ void tile_of(int t, int& ti, int& tj) {
 
 // One pivot of the warp-register factor of a 32x32 diagonal block (lane =
 // row). The pivot index is a template parameter so that every register index
-// is a compile-time constant (the array stays in registers).
+// is a compile-time constant (the array stays in registers). Column J is
+// broadcast through shared memory (one store per lane, broadcast reads);
+// entries right of a lane's diagonal are updated too but never read.
 template <int J>
 __device__ __forceinline__ void chol_step(double (&wr)[CNB], int lane, CholSmem& S, bool& bad) {
-  const double d = __shfl_sync(0xffffffffu, wr[J], J);
+  S.col[lane] = wr[J];
+  __syncwarp();
+  const double d = S.col[J];
   const bool ok = d > 0.0 && isfinite(d);
   const double dd = ok ? d : 1.0;
   const double rs = rsqrt(dd);
@@ -159,10 +159,8 @@ __device__ __forceinline__ void chol_step(double (&wr)[CNB], int lane, CholSmem&
   }
   const double w = lj * (rs * rs);
 #pragma unroll
-  for (int t = J + 1; t < CNB; ++t) {
-    const double ct = __shfl_sync(0xffffffffu, wr[J], t);
-    if (t <= lane) wr[t] -= ct * w;
-  }
+  for (int t = J + 1; t < CNB; ++t) wr[t] = fma(-S.col[t], w, wr[t]);
+  __syncwarp();
   if constexpr (J + 1 < CNB) chol_step<J + 1>(wr, lane, S, bad);
 }
 
@@ -189,7 +187,7 @@ __device__ __forceinline__ void solve_step(double (&x)[CNB], const CholSmem& S) 
 // 256 threads update the tile (four outputs each). The first tile's panel
 // rows are loaded before the factor, so that load overlaps it.
 __global__ void __launch_bounds__(256, 1) k_band_chol(int n, int band, long long ldb, double* A, double* L, int* flag,
-                                                      unsigned* bar_count, unsigned* bar_gen, int* err, int poll) {
+                                                      unsigned* bar_count, int* err, int poll) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   CholSmem& S = *reinterpret_cast<CholSmem*>(smem_raw);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -265,18 +263,22 @@ __global__ void __launch_bounds__(256, 1) k_band_chol(int n, int band, long long
       }
       const int i = i0 + r;
       if (i < lim) {
+        // all four loads before any store (the stores could alias them)
+        double av[4];
+        bool in[4];
 #pragma unroll
         for (int m = 0; m < 4; ++m) {
           const int j = j0 + c0 + m;
-          if (j < lim && j <= i && i - j <= band) {
-            double* a = A + bidx(i, j, band, ldb);
-            *a = ldcg(a) - acc[m];
-          }
+          in[m] = j < lim && j <= i && i - j <= band;
+          av[m] = in[m] ? ldcg(A + bidx(i, j, band, ldb)) : 0.0;
         }
+#pragma unroll
+        for (int m = 0; m < 4; ++m)
+          if (in[m]) A[bidx(i, j0 + c0 + m, band, ldb)] = av[m] - acc[m];
       }
       __syncthreads();
     }
-    if (!grid_barrier(bar_count, bar_gen, gridDim.x, err, poll)) return;
+    if (!grid_barrier(bar_count, (unsigned)(k / CNB + 1), gridDim.x, err, poll)) return;
   }
 }
 
@@ -314,8 +316,9 @@ __global__ void __launch_bounds__(CNB) k_diag_inverse(int n, int band, long long
 // narrower than a row block. A step reads its L rows from L2 (all strips at
 // block row I read the same rows) in 64-wide chunks, the next chunk
 // prefetched into registers. Warp w takes the chunk columns k = w, w+8, ...;
-// lane r keeps row r of the 32 x TWC partial product; the 8 warp partials are
-// summed through shared memory.
+// lane l keeps rows l%16 and l%16+16 of half the strip's columns (6 shared
+// loads per 16 FMA, no bank conflicts); the 8 warp partials are summed
+// through shared memory. The step's diagonal inverse is fetched at its start.
 // W goes to W64 (lower part, FP64) and to the apply matrix (C64 or C32) as W
 // in the lower triangle and W^T in the strict upper triangle, row stride ldc.
 constexpr int TIT = 256, TKC = 64, TWC = 16;
@@ -340,10 +343,15 @@ __global__ void __launch_bounds__(TIT) k_tri_inverse(int n, int band, long long 
   constexpr int PW = TKC * TWC / TIT;  // W values fetched per thread per chunk
   constexpr int PO = CNB * TWC / TIT;  // outputs per thread per step
   static_assert(PL * TIT == CNB * TKC && PW * TIT == TKC * TWC && PO * TIT == CNB * TWC, "tile split");
+  // lane mapping of the partial product: rows rl and rl+16, columns ch .. ch+TWC/2
+  const int rl = lane & 15, ch = (lane >> 4) * (TWC / 2);
   double pl[PL], pw[PW];
+  double dpre[CNB * CNB / TIT];
   for (int I = j0 / CNB; I < nT; ++I) {
     const int i0 = I * CNB;
     const int klo = max(j0, i0 - band);
+#pragma unroll
+    for (int m = 0; m < CNB * CNB / TIT; ++m) dpre[m] = Dinv[(long long)I * CNB * CNB + t + TIT * m];
     auto fetch = [&](int k0) {
 #pragma unroll
       for (int m = 0; m < PL; ++m) {
@@ -379,19 +387,28 @@ __global__ void __launch_bounds__(TIT) k_tri_inverse(int n, int band, long long 
 #pragma unroll 4
       for (int m = 0; m < TKC / 8; ++m) {
         const int kk = warp + 8 * m;
-        const double a = S.Ls[lane][kk];
-        const double2* wr = reinterpret_cast<const double2*>(&S.Wc[kk][0]);
+        const double a0 = S.Ls[rl][kk], a1 = S.Ls[rl + 16][kk];
+        const double2* wr = reinterpret_cast<const double2*>(&S.Wc[kk][ch]);
 #pragma unroll
-        for (int c2 = 0; c2 < TWC / 2; ++c2) {
+        for (int c2 = 0; c2 < TWC / 4; ++c2) {
           const double2 w = wr[c2];
-          acc[2 * c2] = fma(a, w.x, acc[2 * c2]);
-          acc[2 * c2 + 1] = fma(a, w.y, acc[2 * c2 + 1]);
+          acc[2 * c2] = fma(a0, w.x, acc[2 * c2]);
+          acc[2 * c2 + 1] = fma(a0, w.y, acc[2 * c2 + 1]);
+          acc[TWC / 2 + 2 * c2] = fma(a1, w.x, acc[TWC / 2 + 2 * c2]);
+          acc[TWC / 2 + 2 * c2 + 1] = fma(a1, w.y, acc[TWC / 2 + 2 * c2 + 1]);
         }
       }
     }
 #pragma unroll
-    for (int c = 0; c < TWC; ++c) S.red[warp][lane][c] = acc[c];
-    for (int q = t; q < CNB * CNB; q += TIT) S.Ds[q >> 5][q & 31] = Dinv[(long long)I * CNB * CNB + q];
+    for (int c = 0; c < TWC / 2; ++c) {
+      S.red[warp][rl][ch + c] = acc[c];
+      S.red[warp][rl + 16][ch + c] = acc[TWC / 2 + c];
+    }
+#pragma unroll
+    for (int m = 0; m < CNB * CNB / TIT; ++m) {
+      const int q = t + TIT * m;
+      S.Ds[q >> 5][q & 31] = dpre[m];
+    }
     __syncthreads();
 #pragma unroll
     for (int p = 0; p < PO; ++p) {
@@ -604,10 +621,9 @@ void coarsest_factor(CoarsestFactor& f, cudaStream_t s) {
     double* L = f.L;
     int* flag = f.flag;
     unsigned* cnt = f.bar;
-    unsigned* gen = f.bar + 1;
     int* err = f.err;
-    int poll = 1 << 22;
-    void* args[] = {&nn, &band, &ldb, &A, &L, &flag, &cnt, &gen, &err, &poll};
+    int poll = 1 << 24;
+    void* args[] = {&nn, &band, &ldb, &A, &L, &flag, &cnt, &err, &poll};
     TOPO_CUDA_CHECK(cudaLaunchCooperativeKernel((const void*)cst::k_band_chol, dim3(f.chol_grid), dim3(256), args,
                                                 sizeof(cst::CholSmem), s));
     count_launches(1);
