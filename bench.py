@@ -169,8 +169,9 @@ def ku_micro(reps: int = 100, pairs: int = 8):
                      "launches_per_apply": (ctx._lib.topo_launch_count() - n0) / reps}
     out["fp32"]["rel_l2_vs_fp64"] = _rel_l2(first["fp32"], first["fp64"])
     out["bf16"]["rel_l2_vs_fp64"] = _rel_l2(first["bf16"], first["fp64"])
-    out["kernels"] = {"fp64": "k_level0<double> (CUDA cores)", "fp32": "k_level0<float> (CUDA cores)",
-                      "bf16": "k_level0_xs<bf16, Store> (tcgen05, BF16 u, TMA-staged x-planes)"}
+    out["kernels"] = {"fp64": "k_level0_cc<double, Store> (CUDA cores, TMA-staged x-planes)",
+                      "fp32": "k_level0_cc<float, Store> (CUDA cores, TMA-staged x-planes)",
+                      "bf16": "k_level0_xs<bf16, Store> (tcgen05 node-pair tiles, BF16 u, TMA-staged x-planes)"}
     ctx.close()
     return out
 
@@ -217,7 +218,7 @@ def cheb_micro(reps: int = 30, sets: int = 3):
     ms = e0.elapsed_time(e1) / reps
     byts = nd * 28 + ne * 4
     ctx.close()
-    return {"kernel": "k_level0_xs<float, ChebR> (tcgen05, FP32 u rounded to BF16, fused Chebyshev epilogue)",
+    return {"kernel": "k_level0_xs<float, ChebR> (tcgen05 node-pair tiles, FP32 u rounded to BF16, fused Chebyshev epilogue)",
             "workload": "160x80x80 hex8 (3,168,963 DoF), 3 rotating vector sets", "ms": ms, "bytes": byts,
             "gbs": byts / (ms * 1e-3) / 1e9, "gdof_s": nd / (ms * 1e-3) / 1e9}
 

@@ -11,9 +11,10 @@
 //    (window-major) and walks the planes of each window in x: output plane
 //    x reads node planes x-1, x, x+1 and element layers x-1, x, so every
 //    plane is brought in once per run.
-//  * Producer warp (one thread): per node plane one cp.async.bulk (TMA, no
-//    multicast) of the window's 18 node rows of u, per element layer one of
-//    its 17 rows of E, into shared-memory rings completed on mbarriers.
+//  * Producer warp, two threads with streams of their own: per node plane
+//    one cp.async.bulk (TMA, no multicast) of the window's 18 node rows of u,
+//    and per element layer one of its 17 rows of E, into shared-memory rings
+//    completed on mbarriers.
 //    Copies round their start down to 16 bytes; a range ending inside the
 //    last 16 bytes of a vector gets its tail by plain loads, so nothing
 //    outside a vector is read.
@@ -66,7 +67,7 @@ constexpr int W_MMA = W_EPI + W_CONV, W_PROD = W_MMA + 1;
 constexpr int NT = 32 * (W_PROD + 1);  // 16 warps
 constexpr int EPI_T = 32 * W_EPI, CONV_T = 32 * W_CONV, GRP_T = 128;
 constexpr int BTILE = 512;      // bytes of one B tile (16 x 16 BF16)
-constexpr int NBT = 18;         // B tiles (16 x 16 each) of the nine MMAs of a tile
+constexpr int NBT = 18;         // B tiles (16 x 16 each) of the ten MMAs of a tile
 
 // mbarrier indices
 constexpr int B_RAWF = 0, B_RAWE = B_RAWF + NRAW, B_RECF = B_RAWE + NRAW, B_RECE = B_RECF + NREC,
@@ -225,9 +226,10 @@ __device__ __forceinline__ float to_f(TU v) {
 // (ax, ay) = (0,0), (1,0), (1,1), (0,1) at TMEM columns 64*slot + 0, 16, 32,
 // 48; slice column (t, az, c) -> 6t + 3az + c. The A operand (plane x-ax+dx,
 // row y-ay+dy) depends on the plane p in {x-1, x, x+1} and delta = dy-ay only,
-// so nine MMAs cover the 16 (corner, dx, dy) products; each writes the
-// slices its operand feeds (adjacent by the slice order; the (x+1, 0)
-// operand feeds S0 and S3 and carries zero B rows for S1, S2).
+// so nine operands cover the 16 (corner, dx, dy) products; each MMA writes
+// the slices its operand feeds (adjacent by the slice order, except the
+// (x+1, 0) operand, which feeds S0 and S3 in two MMAs; the B tiles between
+// them are zero and unused).
 template <typename TU, Epi EPI>
 __global__ void __launch_bounds__(NT, 1) k_level0_xs(const Params<TU> P) {
   if (P.st != nullptr && P.st->done) return;
@@ -282,59 +284,66 @@ __global__ void __launch_bounds__(NT, 1) k_level0_xs(const Params<TU> P) {
   if (warp == W_PROD) {
     // ------------------------------------------------------------ producer
     if (lane == 0) {
-      long long kr = 0, ke = 0;
+      // node planes of u (raw, converted by the converter warps)
+      long long kr = 0;
       bool ok = true;
       const unsigned char* ub = reinterpret_cast<const unsigned char*>(P.u);
-      const unsigned char* ebp = reinterpret_cast<const unsigned char*>(P.E);
       const long long ubytes = g.ndof * (long long)sizeof(TU);
       while (ok && run.next()) {
         const int ya = max(WY * run.w - 1, 0), yb = min(WY * run.w + WY + 1, NY);  // staged node rows
-        const int ea = max(WY * run.w - 1, 0), eb = min(WY * run.w + WY, g.ny);    // staged element rows
         const int nout = run.xb - run.xa + 1;
         for (int i = 0; i <= nout + 1 && ok; ++i) {
-          {
-            const int Pl = run.xa - 1 + i;
-            const int s = (int)(kr % P.nraw);
-            ok = wait_bar(BAR(B_RAWE + s), (uint32_t)(((kr / P.nraw) & 1) ^ 1), abort_flag, P.err, P.poll);
-            if (!ok) break;
-            unsigned char* dst = sm + P.off_raw + s * P.raw_slot;
-            uint32_t bytes = 0;
-            long long off0 = 0;
-            if (Pl >= 0 && Pl < NX && yb > ya) {
-              off0 = (long long)row3 * ((long long)Pl * NY + ya) * (long long)sizeof(TU);
-              bytes = stage_range(dst, ub, off0, (long long)(yb - ya) * row3 * (long long)sizeof(TU), ubytes);
-            }
-            mbar_arrive_tx(BAR(B_RAWF + s), bytes);
-            issue_range(dst, ub, off0, bytes, BAR(B_RAWF + s));
-            ++kr;
+          const int Pl = run.xa - 1 + i;
+          const int s = (int)(kr % P.nraw);
+          ok = wait_bar(BAR(B_RAWE + s), (uint32_t)(((kr / P.nraw) & 1) ^ 1), abort_flag, P.err, P.poll);
+          if (!ok) break;
+          unsigned char* dst = sm + P.off_raw + s * P.raw_slot;
+          uint32_t bytes = 0;
+          long long off0 = 0;
+          if (Pl >= 0 && Pl < NX && yb > ya) {
+            off0 = (long long)row3 * ((long long)Pl * NY + ya) * (long long)sizeof(TU);
+            bytes = stage_range(dst, ub, off0, (long long)(yb - ya) * row3 * (long long)sizeof(TU), ubytes);
           }
-          if (i <= nout) {
-            const int L = run.xa - 1 + i;
-            const int s = (int)(ke % P.ne);
-            ok = wait_bar(BAR(B_EE + s), (uint32_t)(((ke / P.ne) & 1) ^ 1), abort_flag, P.err, P.poll);
-            if (!ok) break;
-            unsigned char* dst = sm + P.off_e + s * P.e_slot;
-            uint32_t bytes = 0;
-            long long off0 = 0;
-            if (L >= 0 && L < g.nx && eb > ea) {
-              off0 = 4LL * g.nz * ((long long)L * g.ny + ea);
-              bytes = stage_range(dst, ebp, off0, 4LL * (eb - ea) * g.nz, 4LL * g.nelem);
-            }
-            mbar_arrive_tx(BAR(B_EF + s), bytes);
-            issue_range(dst, ebp, off0, bytes, BAR(B_EF + s));
-            ++ke;
-          }
+          mbar_arrive_tx(BAR(B_RAWF + s), bytes);
+          issue_range(dst, ub, off0, bytes, BAR(B_RAWF + s));
+          ++kr;
         }
       }
-      if (!ok) {
-        // drain: wait until the copies already issued have landed
+      if (!ok)  // drain: wait until the copies already issued have landed
         for (long long j = max(0LL, kr - (long long)P.nraw); j < kr; ++j)
           for (int it = 0; it < P.poll && !mbar_try(BAR(B_RAWF + (int)(j % P.nraw)), (uint32_t)((j / P.nraw) & 1)); ++it) {
           }
+    }
+    if (lane == 1) {
+      // element layers of E (a stream of its own, so a full E ring never
+      // holds back the next node plane)
+      long long ke = 0;
+      bool ok = true;
+      const unsigned char* ebp = reinterpret_cast<const unsigned char*>(P.E);
+      while (ok && run.next()) {
+        const int ea = max(WY * run.w - 1, 0), eb = min(WY * run.w + WY, g.ny);  // staged element rows
+        const int nout = run.xb - run.xa + 1;
+        for (int i = 0; i <= nout && ok; ++i) {
+          const int L = run.xa - 1 + i;
+          const int s = (int)(ke % P.ne);
+          ok = wait_bar(BAR(B_EE + s), (uint32_t)(((ke / P.ne) & 1) ^ 1), abort_flag, P.err, P.poll);
+          if (!ok) break;
+          unsigned char* dst = sm + P.off_e + s * P.e_slot;
+          uint32_t bytes = 0;
+          long long off0 = 0;
+          if (L >= 0 && L < g.nx && eb > ea) {
+            off0 = 4LL * g.nz * ((long long)L * g.ny + ea);
+            bytes = stage_range(dst, ebp, off0, 4LL * (eb - ea) * g.nz, 4LL * g.nelem);
+          }
+          mbar_arrive_tx(BAR(B_EF + s), bytes);
+          issue_range(dst, ebp, off0, bytes, BAR(B_EF + s));
+          ++ke;
+        }
+      }
+      if (!ok)
         for (long long j = max(0LL, ke - (long long)P.ne); j < ke; ++j)
           for (int it = 0; it < P.poll && !mbar_try(BAR(B_EF + (int)(j % P.ne)), (uint32_t)((j / P.ne) & 1)); ++it) {
           }
-      }
     }
   } else if (warp >= W_EPI && warp < W_MMA) {
     // ----------------------------------------------------------- converter
@@ -402,9 +411,9 @@ __global__ void __launch_bounds__(NT, 1) k_level0_xs(const Params<TU> P) {
       bool ok = true;
       const uint32_t bB = smem_u32(sm);
       const uint32_t rec0 = smem_u32(sm + P.off_rec);
-      uint64_t bd[NBT];  // B operand starting at each tile
-#pragma unroll
-      for (int i = 0; i < NBT; ++i) bd[i] = make_desc(bB + (uint32_t)(BTILE * i), 128, 256);
+      // B operand starting at tile i: address field + 32 i (512 B per tile)
+      const uint64_t bd0 = make_desc(bB, 128, 256);
+      auto bd = [&](int i) { return bd0 + (uint64_t)(i * (BTILE >> 4)); };
       while (ok && run.next()) {
         const int nout = run.xb - run.xa + 1;
         const long long k0 = kr;  // stream index of node plane xa-1
@@ -420,13 +429,11 @@ __global__ void __launch_bounds__(NT, 1) k_level0_xs(const Params<TU> P) {
           // A descriptors of planes x-1, x, x+1 at row offset delta = -1, 0, 1
           // (K = two consecutive z-pairs, LBO 16 B); a tile adds 8 qt pairs
           // (+16 B each) to the address field
-          uint64_t ad[3][3];
+          uint64_t ab[3];
 #pragma unroll
-          for (int d = 0; d < 3; ++d) {
-            const uint32_t pl = rec0 + (uint32_t)((kp + d) % P.nrec) * (uint32_t)P.rec_slot;
-#pragma unroll
-            for (int dl = 0; dl < 3; ++dl) ad[d][dl] = make_desc(pl + (uint32_t)(dl * CS), 16, CS);
-          }
+          for (int d = 0; d < 3; ++d) ab[d] = make_desc(rec0 + (uint32_t)((kp + d) % P.nrec) * (uint32_t)P.rec_slot, 16, CS);
+          const uint64_t cs16 = (uint64_t)(CS >> 4);
+          auto ad = [&](int d, int dl) { return ab[d] + (uint64_t)dl * cs16; };
           for (int qt = 0; qt < P.NQ && ok; ++qt, ++t) {
             const int ts = (int)(t % TSLOT);
             ok = wait_bar(BAR(B_TE + ts), (uint32_t)(((t / TSLOT) & 1) ^ 1), abort_flag, P.err, P.poll);
@@ -436,15 +443,16 @@ __global__ void __launch_bounds__(NT, 1) k_level0_xs(const Params<TU> P) {
             const uint64_t qa = (uint64_t)(8 * qt);
             // the nine (plane, delta) operands; slices S0..S3 = corners
             // (0,0), (1,0), (1,1), (0,1) at columns 0, 16, 32, 48
-            mma_bf16(d0, ad[1][1] + qa, bd[0], idesc_n(64), 0u);
-            mma_bf16(d0, ad[1][2] + qa, bd[4], idesc_n(32), 1u);
-            mma_bf16(d0 + 32, ad[1][0] + qa, bd[6], idesc_n(32), 1u);
-            mma_bf16(d0, ad[2][1] + qa, bd[8], idesc_n(64), 1u);
-            mma_bf16(d0 + 16, ad[0][1] + qa, bd[12], idesc_n(32), 1u);
-            mma_bf16(d0, ad[2][2] + qa, bd[14], idesc_n(16), 1u);
-            mma_bf16(d0 + 48, ad[2][0] + qa, bd[15], idesc_n(16), 1u);
-            mma_bf16(d0 + 16, ad[0][2] + qa, bd[16], idesc_n(16), 1u);
-            mma_bf16(d0 + 32, ad[0][0] + qa, bd[17], idesc_n(16), 1u);
+            mma_bf16(d0, ad(1, 1) + qa, bd(0), idesc_n(64), 0u);
+            mma_bf16(d0, ad(1, 2) + qa, bd(4), idesc_n(32), 1u);
+            mma_bf16(d0 + 32, ad(1, 0) + qa, bd(6), idesc_n(32), 1u);
+            mma_bf16(d0, ad(2, 1) + qa, bd(8), idesc_n(16), 1u);
+            mma_bf16(d0 + 48, ad(2, 1) + qa, bd(11), idesc_n(16), 1u);
+            mma_bf16(d0 + 16, ad(0, 1) + qa, bd(12), idesc_n(32), 1u);
+            mma_bf16(d0, ad(2, 2) + qa, bd(14), idesc_n(16), 1u);
+            mma_bf16(d0 + 48, ad(2, 0) + qa, bd(15), idesc_n(16), 1u);
+            mma_bf16(d0 + 16, ad(0, 2) + qa, bd(16), idesc_n(16), 1u);
+            mma_bf16(d0 + 32, ad(0, 0) + qa, bd(17), idesc_n(16), 1u);
             mma_commit(BAR(B_TF + ts));
             last_commit = t;
           }
@@ -746,7 +754,7 @@ bool level0_xs_supported(const Grid& g) {
   return xs_layout(g, 4, L);
 }
 
-// B operand: 18 tiles of 16 x 16 BF16 in the order the nine MMAs read
+// B operand: 18 tiles of 16 x 16 BF16 in the order the ten MMAs read
 // them. Tile T(ax, ay, dx, dy): input k = (pair po = k/8, record rr = (k/4)%2,
 // component k%4) is node 2j-1+r (r = 2po + rr) of row y-ay+dy of plane
 // x-ax+dx; output n = (t = n/6, az = (n%6)/3, c = n%3) is component c of node
