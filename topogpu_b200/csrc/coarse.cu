@@ -127,8 +127,11 @@ __host__ __device__ inline PairList rap_pairs(int d) {
 
 __global__ void __launch_bounds__(128) k_rap(Grid f, Grid c, const double* __restrict__ Sf, const uint8_t* __restrict__ mc,
                                              double* __restrict__ Sc) {
-  const int kd = blockIdx.y;  // neighbour offset of the output block, uniform per CTA
-  const long long I = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  // CTA b: neighbour offset kd = b % 27 (uniform per CTA) of coarse nodes
+  // [128 (b / 27), +128); the 27 offsets of a node range are adjacent in
+  // launch order, so they read that range's fine coefficients from L2
+  const int kd = (int)(blockIdx.x % 27);
+  const long long I = (long long)(blockIdx.x / 27) * blockDim.x + threadIdx.x;
   if (I >= c.nnodes) return;
   int Ix, Iy, Iz;
   node_xyz(c, I, Ix, Iy, Iz);
@@ -175,7 +178,7 @@ __global__ void __launch_bounds__(128) k_rap(Grid f, Grid c, const double* __res
 void rap(const Grid& fine, const Grid& coarse, const double* S_f, const uint8_t* mask_c, double* S_c,
          cudaStream_t s) {
   const int bs = 128;
-  k_rap<<<dim3((unsigned)((coarse.nnodes + bs - 1) / bs), 27), bs, 0, s>>>(fine, coarse, S_f, mask_c, S_c);
+  k_rap<<<(unsigned)(27 * ((coarse.nnodes + bs - 1) / bs)), bs, 0, s>>>(fine, coarse, S_f, mask_c, S_c);
   TOPO_LAUNCH_CHECK();
 }
 

@@ -154,6 +154,10 @@ struct Coarsest {
   bool bg_pending = false;  // nxt is being built on bg_stream
   cudaStream_t bg_stream = nullptr;
   cudaEvent_t ev_copy = nullptr, bg_done = nullptr;
+  // set-up side stream: the coarse-level Jacobi diagonals, spectral bounds
+  // and stencil copies run there while the coarsest factorisation runs
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_rap = nullptr, ev_side = nullptr;
   double* tmp = nullptr;   // FP64 Jacobi inverse of a coarse level when vectors are FP32
   double* scrA = nullptr;  // FP64 scratch vectors for the coarse power iterations
   double* scrB = nullptr;
@@ -575,22 +579,23 @@ void do_setup(topo_ctx* c, const double* E, cudaStream_t s) {
     c->lam_Emax = Emax;
   }
   TOPO_CUDA_CHECK(cudaEventRecord(c->ev_ph[1], s));
+  // Galerkin operators of every coarse level first (each R.A.P reads the
+  // level above), then the coarsest factorisation is queued on s and the
+  // per-level Jacobi diagonals, spectral bounds and apply-precision stencil
+  // copies run on the side stream meanwhile: the factorisation keeps at most
+  // one CTA per SM busy on part of the GPU and only reads the coarsest
+  // stencil.
   for (int l = 1; l < c->n_levels; ++l) {
     Level& Lv = c->L[l];
     if (l == 1) level1_assemble(c->L[0].g, Lv.g, c->E64, Lv.mask, Lv.S64, s);
     else rap(c->L[l - 1].g, Lv.g, c->L[l - 1].S64, Lv.mask, Lv.S64, s);
-    if (l == c->n_levels - 1) break;  // coarsest: dense factor below
-    double* dinv64 = c->vec64 ? (double*)Lv.dinv : (double*)c->C.tmp;
-    stencil_dinv(Lv.g, Lv.S64, Lv.mask, dinv64, c->vec64 ? nullptr : (float*)Lv.dinv, s);
-    if (re || std::isnan(Lv.lam)) Lv.lam = lambda_coarse(c, l, dinv64, s);
-    if (Lv.prec == Prec::F32 || Lv.prec == Prec::BF16)
-      stencil_convert(Lv.g.nnodes, Lv.S64, Lv.S32, Lv.prec == Prec::BF16 ? Lv.S16 : nullptr, s);
   }
-  // coarsest: dense FP64 Cholesky + W = L^-1, one graph per factor slot, with
-  // the reference's eps*I retry (multigrid_v4.py:778-811)
   TOPO_CUDA_CHECK(cudaEventRecord(c->ev_ph[2], s));
   TOPO_CUDA_CHECK(cudaEventRecord(c->ev_ph[3], s));
   TOPO_CUDA_CHECK(cudaEventRecord(c->ev_ph[4], s));
+  // coarsest: FP64 band Cholesky + W = L^-1, with the reference's eps*I
+  // retry (multigrid_v4.py:778-811)
+  bool launched_cur = false;
   if (c->n_levels > 1 && c->C.n > 0) {
     Level& Lc = c->L[c->n_levels - 1];
     const size_t sb = sizeof(double) * 243 * Lc.g.nnodes;
@@ -600,8 +605,7 @@ void do_setup(topo_ctx* c, const double* E, cudaStream_t s) {
       TOPO_CUDA_CHECK(cudaEventRecord(c->ev_ph[3], s));
       slot_launch(c, c->C.cur, s);
       TOPO_CUDA_CHECK(cudaEventRecord(c->ev_ph[4], s));
-      slot_finish(c, c->C.cur, s);
-      c->C.have = true;
+      launched_cur = true;
     } else {
       // The V-cycle keeps the previous setup's factor; this setup's factor
       // builds on the background stream and replaces it at the next setup.
@@ -619,6 +623,25 @@ void do_setup(topo_ctx* c, const double* E, cudaStream_t s) {
       TOPO_CUDA_CHECK(cudaEventRecord(c->C.bg_done, c->C.bg_stream));
       c->C.bg_pending = true;
     }
+  }
+  {
+    cudaStream_t t = c->C.side;
+    TOPO_CUDA_CHECK(cudaEventRecord(c->C.ev_rap, s));
+    TOPO_CUDA_CHECK(cudaStreamWaitEvent(t, c->C.ev_rap, 0));
+    for (int l = 1; l < c->n_levels - 1; ++l) {
+      Level& Lv = c->L[l];
+      double* dinv64 = c->vec64 ? (double*)Lv.dinv : (double*)c->C.tmp;
+      stencil_dinv(Lv.g, Lv.S64, Lv.mask, dinv64, c->vec64 ? nullptr : (float*)Lv.dinv, t);
+      if (re || std::isnan(Lv.lam)) Lv.lam = lambda_coarse(c, l, dinv64, t);
+      if (Lv.prec == Prec::F32 || Lv.prec == Prec::BF16)
+        stencil_convert(Lv.g.nnodes, Lv.S64, Lv.S32, Lv.prec == Prec::BF16 ? Lv.S16 : nullptr, t);
+    }
+    TOPO_CUDA_CHECK(cudaEventRecord(c->C.ev_side, t));
+    TOPO_CUDA_CHECK(cudaStreamWaitEvent(s, c->C.ev_side, 0));
+  }
+  if (launched_cur) {
+    slot_finish(c, c->C.cur, s);
+    c->C.have = true;
   }
   TOPO_CUDA_CHECK(cudaEventRecord(c->ev_ph[5], s));
   TOPO_CUDA_CHECK(cudaStreamSynchronize(s));
@@ -1125,6 +1148,9 @@ int topo_ctx_create(int nelx, int nely, int nelz, int n_levels, int mode, int fi
     TOPO_CUDA_CHECK(cudaStreamCreateWithFlags(&c->C.bg_stream, cudaStreamNonBlocking));
     TOPO_CUDA_CHECK(cudaEventCreateWithFlags(&c->C.ev_copy, cudaEventDisableTiming));
     TOPO_CUDA_CHECK(cudaEventCreateWithFlags(&c->C.bg_done, cudaEventDisableTiming));
+    TOPO_CUDA_CHECK(cudaStreamCreateWithFlags(&c->C.side, cudaStreamNonBlocking));
+    TOPO_CUDA_CHECK(cudaEventCreateWithFlags(&c->C.ev_rap, cudaEventDisableTiming));
+    TOPO_CUDA_CHECK(cudaEventCreateWithFlags(&c->C.ev_side, cudaEventDisableTiming));
     int nx = nelx, ny = nely, nz = nelz;
     for (int l = 0; l < n_levels; ++l) {
       Level Lv;
@@ -1210,6 +1236,10 @@ int topo_ctx_destroy(topo_ctx* c) {
   if (c->C.ev_copy) cudaEventDestroy(c->C.ev_copy);
   if (c->C.bg_done) cudaEventDestroy(c->C.bg_done);
   if (c->C.bg_stream) cudaStreamDestroy(c->C.bg_stream);
+  if (c->C.side) cudaStreamSynchronize(c->C.side);
+  if (c->C.ev_rap) cudaEventDestroy(c->C.ev_rap);
+  if (c->C.ev_side) cudaEventDestroy(c->C.ev_side);
+  if (c->C.side) cudaStreamDestroy(c->C.side);
   if (c->ev_in) cudaEventDestroy(c->ev_in);
   if (c->ev_out) cudaEventDestroy(c->ev_out);
   for (auto& e : c->ev_ph)
