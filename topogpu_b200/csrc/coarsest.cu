@@ -6,11 +6,12 @@
 // DoFs. The setup
 //   1. assembles the lower band into band storage,
 //   2. factorises it with one persistent kernel: a right-looking band
-//      Cholesky over 32-column panels with one grid barrier per panel (every
-//      CTA factors the panel's diagonal block in one warp's registers while
-//      two other warps fetch the panel rows of its trailing tile; they solve
-//      them, the CTA updates the tile; the factor goes to a separate band
-//      array so no CTA reads a panel row another CTA has overwritten),
+//      Cholesky over 32-column panels with one grid barrier per panel; the
+//      CTA that updates the next panel's diagonal block factors it in one
+//      warp's registers right away and publishes it (look-ahead), the others
+//      fetch the panel rows of their trailing tiles, solve them in two warps
+//      and update the tile; the factor goes to a separate band array so no
+//      CTA reads a panel row another CTA has overwritten,
 //   3. inverts the 32x32 diagonal blocks of L and forms W = L^-1 by forward
 //      substitution in independent 16-column strips (W is dense lower
 //      triangular; the band of L bounds each step's reads),
@@ -182,55 +183,88 @@ __device__ __forceinline__ void solve_step(double (&x)[CNB], const CholSmem& S) 
   if constexpr (J + 1 < CNB) solve_step<J + 1>(x, S);
 }
 
-// Warps: 0 factors the diagonal block, 2 and 3 solve the panel rows of the
-// two row tiles of each trailing tile (3 only for off-diagonal tiles), all
-// 256 threads update the tile (four outputs each). The first tile's panel
-// rows are loaded before the factor, so that load overlaps it.
-__global__ void __launch_bounds__(256, 1) k_band_chol(int n, int band, long long ldb, double* A, double* L, int* flag,
-                                                      unsigned* bar_count, int* err, int poll) {
+// Warp 0 factors S.W into S.Ld and the reciprocal pivots S.invd; S.bad is
+// set when a pivot was not positive (it is then taken as 1).
+__device__ __forceinline__ void factor_block(CholSmem& S, int warp, int lane) {
+  if (warp == 0) {
+    double wr[CNB];
+#pragma unroll
+    for (int t = 0; t < CNB; ++t) wr[t] = S.W[lane][t];
+    bool bad = false;
+    chol_step<0>(wr, lane, S, bad);
+    bad = __any_sync(0xffffffffu, bad);
+    if (lane == 0) S.bad = bad ? 1 : 0;
+  }
+}
+
+// Warps: 0 factors diagonal blocks, 2 and 3 solve the panel rows of the two
+// row tiles of each trailing tile (3 only for off-diagonal tiles), all 256
+// threads update the tile (four outputs each). Look-ahead (band >= 32):
+// tile 0 of panel k's trailing update, which CTA 0 owns, is panel k+1's
+// diagonal block; CTA 0 keeps its updated values, factors them after its
+// tiles and publishes the factor and pivots in Lnext (double-buffered by
+// panel parity) before the barrier, so at panel k+1 the other CTAs load it
+// instead of factoring, and the panel rows they prefetch meanwhile are the
+// only load in front of their solves. Panel 0, and every panel when the
+// band is narrower than a panel, is factored by every CTA from A.
+__global__ void __launch_bounds__(256, 1) k_band_chol(int n, int band, long long ldb, double* A, double* L,
+                                                      double* Lnext, int* flag, unsigned* bar_count, int* err,
+                                                      int poll) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   CholSmem& S = *reinterpret_cast<CholSmem*>(smem_raw);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const bool solver = warp == 2 || warp == 3;
+  const bool ahead = band >= CNB;
+  constexpr int LN = CNB * (CNB + 1) + CNB;  // one published factor: Ld rows, then pivots
   for (int k = 0; k < n; k += CNB) {
     const int nb = min(CNB, n - k);
     const int base = k + nb;
     const int lim = min(n, base + band);
     const int nt = (lim - base + CNB - 1) / CNB;
     const int ntiles = lim > base ? nt * (nt + 1) / 2 : 0;
-    // 1. diagonal block (identity-padded past n) and the first tile's panel rows
-    for (int q = tid; q < CNB * CNB; q += blockDim.x) {
-      const int i = q / CNB, j = q % CNB;
-      S.W[i][j] = (i < nb && j < nb && j <= i) ? (i - j <= band ? ldcg(A + bidx(k + i, k + j, band, ldb)) : 0.0)
-                                               : (i == j ? 1.0 : 0.0);
-    }
-    double x[CNB];
-    if (solver && (int)blockIdx.x < ntiles) {
-      int ti, tj;
-      tile_of(blockIdx.x, ti, tj);
-      const int r0 = warp == 2 ? base + CNB * ti : base + CNB * tj;
-      panel_load(A, band, ldb, k, nb, r0 + lane, lim, x);
-    }
-    __syncthreads();
-    // 2. factor (every CTA does the same arithmetic, so all agree)
-    if (warp == 0) {
-      double wr[CNB];
-#pragma unroll
-      for (int t = 0; t < CNB; ++t) wr[t] = S.W[lane][t];
-      bool bad = false;
-      chol_step<0>(wr, lane, S, bad);
-      bad = __any_sync(0xffffffffu, bad);
-      if (lane == 0) S.bad = bad ? 1 : 0;
-    }
-    __syncthreads();
-    if (blockIdx.x == 0) {
+    const int par = (k / CNB) & 1;
+    const bool own = ahead && k > 0;  // this panel's factor came from the look-ahead
+    // 1. this panel's factored diagonal block and the first tile's panel rows
+    if (!own) {
       for (int q = tid; q < CNB * CNB; q += blockDim.x) {
         const int i = q / CNB, j = q % CNB;
-        if (i < nb && j <= i && i - j <= band) L[bidx(k + i, k + j, band, ldb)] = S.Ld[i][j];
+        S.W[i][j] = (i < nb && j < nb && j <= i) ? (i - j <= band ? ldcg(A + bidx(k + i, k + j, band, ldb)) : 0.0)
+                                                 : (i == j ? 1.0 : 0.0);
       }
-      if (tid == 0 && S.bad) *flag = 1;
+    } else if (blockIdx.x != 0) {
+      const double* src = Lnext + par * LN;
+      for (int q = tid; q < CNB * (CNB + 1); q += blockDim.x) (&S.Ld[0][0])[q] = ldcg(src + q);
+      if (tid < CNB) S.invd[tid] = ldcg(src + CNB * (CNB + 1) + tid);
     }
-    // 3. trailing tiles of the band window
+    double x[CNB];
+    const int r = tid >> 3, c0 = (tid & 7) * 4;  // this thread's four outputs of a trailing tile
+    double a0[4] = {0.0, 0.0, 0.0, 0.0};        // their current values for the first tile
+    if ((int)blockIdx.x < ntiles) {
+      int ti, tj;
+      tile_of(blockIdx.x, ti, tj);
+      if (solver) panel_load(A, band, ldb, k, nb, (warp == 2 ? base + CNB * ti : base + CNB * tj) + lane, lim, x);
+      const int i = base + CNB * ti + r;
+#pragma unroll
+      for (int m = 0; m < 4; ++m) {
+        const int j = base + CNB * tj + c0 + m;
+        if (i < lim && j < lim && j <= i && i - j <= band) a0[m] = ldcg(A + bidx(i, j, band, ldb));
+      }
+    }
+    __syncthreads();
+    if (!own) {
+      // every CTA does the same arithmetic, so all agree
+      factor_block(S, warp, lane);
+      __syncthreads();
+      if (blockIdx.x == 0) {
+        for (int q = tid; q < CNB * CNB; q += blockDim.x) {
+          const int i = q / CNB, j = q % CNB;
+          if (i < nb && j <= i && i - j <= band) L[bidx(k + i, k + j, band, ldb)] = S.Ld[i][j];
+        }
+        if (tid == 0 && S.bad) *flag = 1;
+      }
+    }
+    // 2. trailing tiles of the band window
+    const bool la = ahead && blockIdx.x == 0 && base < n;  // CTA 0 builds panel k+1's block in S.W
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
       int ti, tj;
       tile_of(t, ti, tj);
@@ -253,7 +287,6 @@ __global__ void __launch_bounds__(256, 1) k_band_chol(int n, int band, long long
           if (i < lim && j < nb && i - (k + j) <= band) L[bidx(i, k + j, band, ldb)] = S.Pi[r][j];
         }
       }
-      const int r = tid >> 3, c0 = (tid & 7) * 4;
       double acc[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll 8
       for (int q = 0; q < CNB; ++q) {
@@ -262,21 +295,39 @@ __global__ void __launch_bounds__(256, 1) k_band_chol(int n, int band, long long
         for (int m = 0; m < 4; ++m) acc[m] = fma(li, Pj[c0 + m][q], acc[m]);
       }
       const int i = i0 + r;
-      if (i < lim) {
-        // all four loads before any store (the stores could alias them)
-        double av[4];
-        bool in[4];
+      const bool blk = la && t == 0;  // tile 0 = panel k+1's diagonal block
+      // all four loads before any store (the stores could alias them)
+      double av[4];
+      bool in[4];
 #pragma unroll
-        for (int m = 0; m < 4; ++m) {
-          const int j = j0 + c0 + m;
-          in[m] = j < lim && j <= i && i - j <= band;
-          av[m] = in[m] ? ldcg(A + bidx(i, j, band, ldb)) : 0.0;
-        }
+      for (int m = 0; m < 4; ++m) {
+        const int j = j0 + c0 + m;
+        in[m] = i < lim && j < lim && j <= i && i - j <= band;
+        const double cur = t == (int)blockIdx.x ? a0[m] : (in[m] ? ldcg(A + bidx(i, j, band, ldb)) : 0.0);
+        av[m] = in[m] ? cur - acc[m] : 0.0;
+      }
 #pragma unroll
-        for (int m = 0; m < 4; ++m)
-          if (in[m]) A[bidx(i, j0 + c0 + m, band, ldb)] = av[m] - acc[m];
+      for (int m = 0; m < 4; ++m) {
+        if (in[m]) A[bidx(i, j0 + c0 + m, band, ldb)] = av[m];
+        // band >= 32: every entry of the block on or below the diagonal and
+        // below row n is in the window; rows past n are identity-padded
+        if (blk) S.W[r][c0 + m] = in[m] ? av[m] : ((i >= n && r == c0 + m) ? 1.0 : 0.0);
       }
       __syncthreads();
+    }
+    if (la) {
+      // 3. look-ahead: factor panel k+1's block, publish it, write its L block
+      factor_block(S, warp, lane);
+      __syncthreads();
+      const int nb1 = min(CNB, n - base);
+      double* dst = Lnext + (par ^ 1) * LN;
+      for (int q = tid; q < CNB * (CNB + 1); q += blockDim.x) dst[q] = (&S.Ld[0][0])[q];
+      if (tid < CNB) dst[CNB * (CNB + 1) + tid] = S.invd[tid];
+      for (int q = tid; q < CNB * CNB; q += blockDim.x) {
+        const int i = q / CNB, j = q % CNB;
+        if (i < nb1 && j <= i && i - j <= band) L[bidx(base + i, base + j, band, ldb)] = S.Ld[i][j];
+      }
+      if (tid == 0 && S.bad) *flag = 1;
     }
     if (!grid_barrier(bar_count, (unsigned)(k / CNB + 1), gridDim.x, err, poll)) return;
   }
@@ -568,6 +619,7 @@ void coarsest_alloc(CoarsestFactor& f, const CoarsestPlan& p, int band, bool f64
   f.A = (double*)A(nbs * sizeof(double));
   f.L = (double*)A(nbs * sizeof(double));
   f.Dinv = (double*)A((size_t)std::max(p.nt, 1) * cst::CNB * cst::CNB * sizeof(double));
+  f.Lnext = (double*)A(2 * (size_t)(cst::CNB * (cst::CNB + 1) + cst::CNB) * sizeof(double));
   f.ldc = ((long long)n + 31) / 32 * 32;
   f.W64 = (double*)A((size_t)n * f.ldc * sizeof(double));
   f.C = f64 ? (void*)f.W64 : A((size_t)n * f.ldc * sizeof(float));
@@ -619,11 +671,12 @@ void coarsest_factor(CoarsestFactor& f, cudaStream_t s) {
     long long ldb = f.ldb;
     double* A = f.A;
     double* L = f.L;
+    double* Ln = f.Lnext;
     int* flag = f.flag;
     unsigned* cnt = f.bar;
     int* err = f.err;
     int poll = 1 << 24;
-    void* args[] = {&nn, &band, &ldb, &A, &L, &flag, &cnt, &err, &poll};
+    void* args[] = {&nn, &band, &ldb, &A, &L, &Ln, &flag, &cnt, &err, &poll};
     TOPO_CUDA_CHECK(cudaLaunchCooperativeKernel((const void*)cst::k_band_chol, dim3(f.chol_grid), dim3(256), args,
                                                 sizeof(cst::CholSmem), s));
     count_launches(1);

@@ -277,6 +277,7 @@ void op_apply(topo_ctx* c, int l, Prec p, const void* u, void* y, Epi epi, const
 
 // Precision of the one update per V-cycle applied to a smooth vector (the
 // prolongated correction): a BF16-input level uses its FP32 operator there.
+
 Prec hi_prec(const Level& Lv) { return Lv.prec == Prec::BF16 ? Prec::F32 : Lv.prec; }
 
 // Chebyshev-Jacobi smoothing on level l (reference: multigrid_v4.py:861-889)
@@ -349,6 +350,9 @@ void vcycle(topo_ctx* c, int l, const KrylovState* st, cudaStream_t s) {
     ea.r = Lv.r;
     ea.s = 1.0;
     ea.st = const_cast<KrylovState*>(st);
+    // r -= K e in FP32 even where the level's operator is BF16: the
+    // post-smoother continues from this recursive residual, and BF16 here
+    // raised the PCG iterations of the 1M-element cantilever from ~18 to ~95
     op_apply(c, l, hi_prec(Lv), Lv.e, nullptr, Epi::RUpd, ea, s);  // r -= K e
   }
   smooth(c, l, false, false, st, s);

@@ -262,6 +262,7 @@ struct CoarsestFactor {
   bool f64 = true;                          // apply matrix and vectors in FP64 (else FP32)
   double *A = nullptr, *L = nullptr;        // band storage (n x (band+1)): operator, factor
   double* Dinv = nullptr;                   // inverses of the 32x32 diagonal blocks of L
+  double* Lnext = nullptr;                  // look-ahead: the next panel's factored block (two slots)
   double* W64 = nullptr;                    // W = L^-1 (lower triangle, row stride ldc)
   void* C = nullptr;                        // apply matrix: W below, W^T above (W64 itself in FP64)
   long long ldc = 0;
