@@ -525,6 +525,42 @@ __global__ void k_coarse_gather(int n, long long nfull, const int* __restrict__ 
   }
 }
 
+// Warp dot product sum_{j in [lo, hi)} Ci[j] v[j] of one row: 16-byte loads
+// from a V-aligned start, four in flight per lane. Every load begins below
+// hi <= n <= ldc at a multiple of V, and ldc is a multiple of 32, so none
+// leaves the row's storage; entries outside [lo, hi) are not used.
+template <typename TX>
+__device__ __forceinline__ double row_dot(const TX* __restrict__ Ci, const double* __restrict__ v, int lo, int hi,
+                                          int lane) {
+  constexpr int V = 16 / sizeof(TX);
+  constexpr int U = 4;
+  double acc = 0.0;
+  int j = (lo / V) * V + lane * V;
+  for (; j + (U - 1) * 32 * V < hi; j += U * 32 * V) {
+    TX w[U][V];
+#pragma unroll
+    for (int u = 0; u < U; ++u) *reinterpret_cast<uint4*>(w[u]) = __ldg(reinterpret_cast<const uint4*>(Ci + j + u * 32 * V));
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+#pragma unroll
+      for (int q = 0; q < V; ++q) {
+        const int jj = j + u * 32 * V + q;
+        if (jj >= lo && jj < hi) acc += (double)w[u][q] * __ldg(v + jj);
+      }
+  }
+  for (; j < hi; j += 32 * V) {
+    TX w[V];
+    *reinterpret_cast<uint4*>(w) = __ldg(reinterpret_cast<const uint4*>(Ci + j));
+#pragma unroll
+    for (int q = 0; q < V; ++q) {
+      const int jj = j + q;
+      if (jj >= lo && jj < hi) acc += (double)w[q] * __ldg(v + jj);
+    }
+  }
+  return warp_sum(acc);
+}
+
+// pass one: y = W r_c (row i reads C[i][0..i])
 template <typename TX>
 __global__ void __launch_bounds__(256) k_coarse_lower(int n, long long ldc, const TX* __restrict__ C,
                                                       const double* __restrict__ rc, double* __restrict__ y,
@@ -532,34 +568,11 @@ __global__ void __launch_bounds__(256) k_coarse_lower(int n, long long ldc, cons
   if (st != nullptr && st->done) return;
   const int row = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
   if (row >= n) return;
-  constexpr int V = 16 / sizeof(TX);
-  const TX* Ci = C + (long long)row * ldc;
-  double acc = 0.0;
-  int j = lane * V;
-  for (; j + 32 * V <= row; j += 64 * V) {  // two 16-byte loads in flight
-    TX v[V], w[V];
-    *reinterpret_cast<uint4*>(v) = __ldg(reinterpret_cast<const uint4*>(Ci + j));
-    const bool two = j + 32 * V <= row;
-    if (two) *reinterpret_cast<uint4*>(w) = __ldg(reinterpret_cast<const uint4*>(Ci + j + 32 * V));
-#pragma unroll
-    for (int q = 0; q < V; ++q) acc += (double)v[q] * __ldg(rc + j + q);
-    if (two) {
-#pragma unroll
-      for (int q = 0; q < V; ++q)
-        if (j + 32 * V + q <= row) acc += (double)w[q] * __ldg(rc + j + 32 * V + q);
-    }
-  }
-  for (; j <= row; j += 32 * V) {
-    TX v[V];
-    *reinterpret_cast<uint4*>(v) = __ldg(reinterpret_cast<const uint4*>(Ci + j));
-#pragma unroll
-    for (int q = 0; q < V; ++q)
-      if (j + q <= row) acc += (double)v[q] * __ldg(rc + j + q);
-  }
-  acc = warp_sum(acc);
+  const double acc = row_dot(C + (long long)row * ldc, rc, 0, row + 1, lane);
   if (lane == 0) y[row] = acc;
 }
 
+// pass two: z_c = W^T y (row j reads C[j][j..n-1]), scattered to the free DoFs
 template <typename T, typename TX>
 __global__ void __launch_bounds__(256) k_coarse_upper(int n, long long nfull, long long ldc, const TX* __restrict__ C,
                                                       const int* __restrict__ free_list,
@@ -568,29 +581,7 @@ __global__ void __launch_bounds__(256) k_coarse_upper(int n, long long nfull, lo
   if (st != nullptr && st->done) return;
   const int row = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
   if (row >= n) return;
-  constexpr int V = 16 / sizeof(TX);
-  const TX* Cj = C + (long long)row * ldc;
-  double acc = 0.0;
-  int i = (row / V) * V + lane * V;
-  for (; i + 32 * V < n; i += 64 * V) {  // two 16-byte loads in flight
-    TX v[V], w[V];
-    *reinterpret_cast<uint4*>(v) = __ldg(reinterpret_cast<const uint4*>(Cj + i));
-    *reinterpret_cast<uint4*>(w) = __ldg(reinterpret_cast<const uint4*>(Cj + i + 32 * V));
-#pragma unroll
-    for (int q = 0; q < V; ++q)
-      if (i + q >= row) acc += (double)v[q] * __ldg(y + i + q);
-#pragma unroll
-    for (int q = 0; q < V; ++q)
-      if (i + 32 * V + q < n) acc += (double)w[q] * __ldg(y + i + 32 * V + q);
-  }
-  for (; i < n; i += 32 * V) {
-    TX v[V];
-    *reinterpret_cast<uint4*>(v) = __ldg(reinterpret_cast<const uint4*>(Cj + i));
-#pragma unroll
-    for (int q = 0; q < V; ++q)
-      if (i + q >= row && i + q < n) acc += (double)v[q] * __ldg(y + i + q);
-  }
-  acc = warp_sum(acc);
+  const double acc = row_dot(C + (long long)row * ldc, y, row, n, lane);
   if (lane == 0) {
     const int f = free_list[row];
     if (topo_in_range(f, nfull)) x[f] = (T)acc;
