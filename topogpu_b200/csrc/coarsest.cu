@@ -383,12 +383,19 @@ struct TriSmem {
 
 __global__ void __launch_bounds__(TIT) k_tri_inverse(int n, int band, long long ldb, const double* __restrict__ L,
                                                      const double* __restrict__ Dinv, double* W64, long long ldc,
-                                                     double* C64, float* C32) {
+                                                     double* C64, float* C32, int wave) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   TriSmem& S = *reinterpret_cast<TriSmem*>(smem_raw);
   const int nT = (n + CNB - 1) / CNB;
   const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
-  const int j0 = blockIdx.x * TWC;
+  // Strip s takes about nT - s/2 steps. Blocks are placed on the SMs breadth
+  // first (`wave` per pass), three per SM, so block b runs beside b +- wave:
+  // the middle pass takes its strips in reverse order, which gives every SM
+  // one long, one middle and one short strip instead of the first SMs the
+  // three longest.
+  int sidx = blockIdx.x;
+  if (wave > 0 && (int)blockIdx.x >= wave && (int)blockIdx.x < 2 * wave) sidx = 3 * wave - 1 - (int)blockIdx.x;
+  const int j0 = sidx * TWC;
   if (j0 >= n) return;  // uniform over the CTA
   constexpr int PL = CNB * TKC / TIT;  // L values fetched per thread per chunk
   constexpr int PW = TKC * TWC / TIT;  // W values fetched per thread per chunk
@@ -626,6 +633,7 @@ void coarsest_alloc(CoarsestFactor& f, const CoarsestPlan& p, int band, bool f64
   TOPO_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cst::k_band_chol, 256, sizeof(cst::CholSmem)));
   const int tiles_max = ((band + cst::CNB - 1) / cst::CNB) * ((band + cst::CNB - 1) / cst::CNB + 1) / 2;
   f.chol_grid = std::max(1, std::min(std::min(nsm * std::max(per_sm, 1), nsm), std::max(tiles_max, 1)));
+  f.nsm = nsm;
   TOPO_CUDA_CHECK(cudaFuncSetAttribute(cst::k_tri_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)sizeof(cst::TriSmem)));
   f.plan = p;
@@ -675,7 +683,8 @@ void coarsest_factor(CoarsestFactor& f, cudaStream_t s) {
   cst::k_diag_inverse<<<p.nt, cst::CNB, 0, s>>>(n, f.band, f.ldb, f.L, f.Dinv);
   TOPO_LAUNCH_CHECK();
   cst::k_tri_inverse<<<(n + cst::TWC - 1) / cst::TWC, cst::TIT, sizeof(cst::TriSmem), s>>>(
-      n, f.band, f.ldb, f.L, f.Dinv, f.W64, f.ldc, f.f64 ? f.W64 : nullptr, f.f64 ? nullptr : (float*)f.C);
+      n, f.band, f.ldb, f.L, f.Dinv, f.W64, f.ldc, f.f64 ? f.W64 : nullptr, f.f64 ? nullptr : (float*)f.C,
+      (n + cst::TWC - 1) / cst::TWC >= 3 * f.nsm ? f.nsm : 0);
   TOPO_LAUNCH_CHECK();
 }
 

@@ -208,23 +208,51 @@ __device__ __forceinline__ double ocf_candidate(double rho, double dc, double dv
   return rn;
 }
 
-__global__ void k_ocf_pass(long long n, const double* __restrict__ rho, const double* __restrict__ dc,
-                           const double* __restrict__ dv, const double* __restrict__ colsum, double volfrac,
-                           double move, double rho_min, double* st, RedWork red) {
+// Three bisection levels per pass: the 7 midpoints of the next three levels
+// of the interval tree [l1, l2] are formed with the operations the
+// sequential bisection would use (node q's children 2q+1 = left half, 2q+2 =
+// right half, each midpoint 0.5 * (lo + hi) of that node's bounds), their
+// volumes summed in one sweep over the elements (each by the same grid
+// reduction as a single-candidate pass, so bit-identical), and the walk down
+// the tree takes the sequential path: evaluation count, last multiplier and
+// bounds are those of one level per pass.
+__global__ void k_ocf_pass3(long long n, const double* __restrict__ rho, const double* __restrict__ dc,
+                            const double* __restrict__ dv, const double* __restrict__ colsum, double volfrac,
+                            double move, double rho_min, double* st, RedWork red) {
   if (st[OF_DONE] != 0.0) return;
-  const double lm = st[OF_LM];
-  double v[1] = {0.0};
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-    v[0] += ocf_candidate(rho[i], dc[i], dv[i], lm, move, rho_min) * colsum[i];
-  double tot[1];
-  if (grid_sum<1>(v, red, tot) && threadIdx.x == 0) {
-    st[OF_EVALS] += 1.0;
-    if (tot[0] / (double)n > volfrac) st[OF_L1] = lm;
-    else st[OF_L2] = lm;
-    st[OF_LAST] = lm;
-    st[OF_K] += 1.0;
-    if (st[OF_L2] - st[OF_L1] < 1e-9 || st[OF_K] >= 100.0) st[OF_DONE] = 1.0;
-    else st[OF_LM] = 0.5 * (st[OF_L1] + st[OF_L2]);
+  const double l1 = st[OF_L1], l2 = st[OF_L2];
+  double c[7];
+  c[0] = 0.5 * (l1 + l2);
+  c[1] = 0.5 * (l1 + c[0]);
+  c[2] = 0.5 * (c[0] + l2);
+  c[3] = 0.5 * (l1 + c[1]);
+  c[4] = 0.5 * (c[1] + c[0]);
+  c[5] = 0.5 * (c[0] + c[2]);
+  c[6] = 0.5 * (c[2] + l2);
+  double v[7] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const double r = rho[i], d = dc[i], w = dv[i], cs = colsum[i];
+#pragma unroll
+    for (int q = 0; q < 7; ++q) v[q] += ocf_candidate(r, d, w, c[q], move, rho_min) * cs;
+  }
+  double tot[7];
+  if (grid_sum<7>(v, red, tot) && threadIdx.x == 0) {
+    int q = 0;
+    for (int level = 0; level < 3; ++level) {
+      const double lm = c[q];
+      st[OF_EVALS] += 1.0;
+      const bool up = tot[q] / (double)n > volfrac;
+      if (up) st[OF_L1] = lm;
+      else st[OF_L2] = lm;
+      st[OF_LAST] = lm;
+      st[OF_K] += 1.0;
+      if (st[OF_L2] - st[OF_L1] < 1e-9 || st[OF_K] >= 100.0) {
+        st[OF_DONE] = 1.0;
+        break;
+      }
+      st[OF_LM] = 0.5 * (st[OF_L1] + st[OF_L2]);
+      q = 2 * q + (up ? 2 : 1);
+    }
   }
 }
 
@@ -250,17 +278,18 @@ int oc_update_filtered(long long n, const double* rho, const double* dc, const d
   TOPO_LAUNCH_CHECK();
   const unsigned nb = (unsigned)std::min<long long>(kRedBlocks, (n + kRedThreads - 1) / kRedThreads);
   auto pass = [&]() {
-    k_ocf_pass<<<nb, kRedThreads, 0, s>>>(n, rho, dc, dv, colsum, volfrac, move, rho_min, st, red);
+    k_ocf_pass3<<<nb, kRedThreads, 0, s>>>(n, rho, dc, dv, colsum, volfrac, move, rho_min, st, red);
     TOPO_LAUNCH_CHECK();
   };
+  // three levels per pass: 34 passes cover the 100-level cap
   double h[16];
   int launched = 0;
   while (true) {
-    for (int k = 0; k < 16 && launched < 100; ++k, ++launched) pass();
+    for (int k = 0; k < 8 && launched < 34; ++k, ++launched) pass();
     TOPO_CUDA_CHECK(cudaMemcpyAsync(h, st, sizeof(double) * 16, cudaMemcpyDeviceToHost, s));
     TOPO_CUDA_CHECK(cudaStreamSynchronize(s));
     if (h[OF_DONE] != 0.0) break;
-    if (launched >= 100) throw std::runtime_error("filtered OC bisection did not terminate");
+    if (launched >= 34) throw std::runtime_error("filtered OC bisection did not terminate");
   }
   k_ocf_final<<<nb, kRedThreads, 0, s>>>(n, rho, dc, dv, move, rho_min, st, out);
   TOPO_LAUNCH_CHECK();

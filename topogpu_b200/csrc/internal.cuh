@@ -270,6 +270,7 @@ struct CoarsestFactor {
   int* err = nullptr;
   unsigned* bar = nullptr;
   int chol_grid = 1;
+  int nsm = 0;                              // SMs of the device (W strip placement)
   const int* d_free = nullptr;
   int kind = 0;                             // 0 none, 1 Cholesky, 2 Cholesky of K + eps I
 };
