@@ -12,19 +12,29 @@
 //      fetch the panel rows of their trailing tiles, solve them in two warps
 //      and update the tile; the factor goes to a separate band array so no
 //      CTA reads a panel row another CTA has overwritten,
-//   3. inverts the 32x32 diagonal blocks of L and forms W = L^-1 by forward
-//      substitution in independent 16-column strips (W is dense lower
-//      triangular; the band of L bounds each step's reads),
-//   4. stores W (lower triangle) and W^T (strict upper triangle) in one
-//      row-major matrix C in the apply precision.
-// The apply z = K^-1 r = W^T (W r) is two bandwidth-bound passes over C, one
-// warp per row, each reading a row contiguously.
+//   3. splits the rows into P diagonal blocks (boundaries on 32-row panels,
+//      each block at least `band` rows, so L is block bidiagonal and block
+//      q+1 reaches block q only through a band x band corner), inverts the
+//      32x32 diagonal blocks of L and forms W_q = L_qq^-1 for every block by
+//      forward substitution in independent 16-column strips (a strip is at
+//      most m/32 steps long instead of n/32),
+//   4. folds the corners through W_q into G_q = W_q Lc_q and
+//      H_q = (Lc_{q+1} W_q[last band rows])^T (FP64 products),
+//   5. stores per block W_q (lower triangle), W_q^T (strict upper triangle),
+//      G_q and H_q in one row-major matrix in the apply precision.
+// The apply z = K^-1 r runs the two triangular solves block by block: a
+// lower pass y_q = W_q r_q - G_q y_{q-1}[tail] for q = 0 .. P-1 and an upper
+// pass z_q = W_q^T y_q - H_q z_{q+1}[head] for q = P-1 .. 0, each a
+// bandwidth-bound product, one warp per row. It reads the P diagonal blocks
+// and their couplings (about n^2/P + 2 n band entries) instead of the n^2 of
+// the dense W^T W.
 //
 // Reference: the coarsest solve of GalerkinMatFreeGMG (src/gpu_fem/
 // multigrid_v4.py:774-811, 969-984): dense Cholesky with an eps*I retry when a
 // pivot is not positive, and two triangular solves per application. The
 // factor here is the same (a band Cholesky creates no fill outside the band);
-// the triangular solves become products with the explicit inverse.
+// the triangular solves become products with the explicit inverses of the
+// diagonal blocks.
 #include "internal.cuh"
 #include "reduce.cuh"
 
@@ -356,22 +366,24 @@ __global__ void __launch_bounds__(CNB) k_diag_inverse(int n, int band, long long
   for (int r = 0; r < CNB; ++r) Dinv[(long long)I * CNB * CNB + r * CNB + c] = X[r][c];
 }
 
-// W = L^-1 by forward substitution, one strip of TWC columns per CTA. Every
-// column of W is an independent forward substitution, so the strips need no
-// communication: CTA J owns columns [TWC J, TWC J + TWC) and walks the
-// 32-row blocks I from the one holding its first column to the last:
+// W_q = L_qq^-1 for every diagonal block q by forward substitution, one strip
+// of TWC columns per CTA. Every column is an independent forward substitution
+// inside its block, so the strips need no communication: a strip with first
+// column j0 walks the 32-row blocks I from the one holding j0 to the end of
+// its diagonal block:
 //   R    = E - sum_{k in [max(j0, 32I-band), 32I)} L[32I.., k] W[k, strip]
 //   W_I  = Dinv_I R                    (E: the identity on these rows/columns)
 // Every W read is of rows this CTA wrote in an earlier step (visible after
-// __syncthreads). The strip of column 0 is the critical path, so strips are
-// narrower than a row block. A step reads its L rows from L2 (all strips at
-// block row I read the same rows) in 64-wide chunks, the next chunk
-// prefetched into registers. Warp w takes the chunk columns k = w, w+8, ...;
-// lane l keeps rows l%16 and l%16+16 of half the strip's columns (6 shared
-// loads per 16 FMA, no bank conflicts); the 8 warp partials are summed
-// through shared memory. The step's diagonal inverse is fetched at its start.
-// W goes to W64 (lower part, FP64) and to the apply matrix (C64 or C32) as W
-// in the lower triangle and W^T in the strict upper triangle, row stride ldc.
+// __syncthreads). A strip takes (block end - j0)/32 steps; CTA r takes strip
+// r/P of block r%P, so the longest strips of all blocks start first. A step
+// reads its L rows from L2 (all strips at block row I read the same rows) in
+// 64-wide chunks, the next chunk prefetched into registers. Warp w takes the
+// chunk columns k = w, w+8, ...; lane l keeps rows l%16 and l%16+16 of half
+// the strip's columns (6 shared loads per 16 FMA, no bank conflicts); the 8
+// warp partials are summed through shared memory. The step's diagonal inverse
+// is fetched at its start. W_q goes to W64 (lower part, FP64) and to the
+// apply matrix (C64 or C32) as W_q in the lower triangle and W_q^T in the
+// strict upper triangle of the block's columns 0 .. m-1.
 constexpr int TIT = 256, TKC = 64, TWC = 16;
 struct TriSmem {
   double Ls[CNB][TKC + 1];
@@ -382,21 +394,20 @@ struct TriSmem {
 };
 
 __global__ void __launch_bounds__(TIT) k_tri_inverse(int n, int band, long long ldb, const double* __restrict__ L,
-                                                     const double* __restrict__ Dinv, double* W64, long long ldc,
-                                                     double* C64, float* C32, int wave) {
+                                                     const double* __restrict__ Dinv, CoarseBlocks bk, double* W64,
+                                                     double* C64, float* C32) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   TriSmem& S = *reinterpret_cast<TriSmem*>(smem_raw);
-  const int nT = (n + CNB - 1) / CNB;
   const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
-  // Strip s takes about nT - s/2 steps. Blocks are placed on the SMs breadth
-  // first (`wave` per pass), three per SM, so block b runs beside b +- wave:
-  // the middle pass takes its strips in reverse order, which gives every SM
-  // one long, one middle and one short strip instead of the first SMs the
-  // three longest.
-  int sidx = blockIdx.x;
-  if (wave > 0 && (int)blockIdx.x >= wave && (int)blockIdx.x < 2 * wave) sidx = 3 * wave - 1 - (int)blockIdx.x;
-  const int j0 = sidx * TWC;
-  if (j0 >= n) return;  // uniform over the CTA
+  const int blk = (int)blockIdx.x % bk.P;
+  const int b0 = bk.b[blk], iend = bk.b[blk + 1];
+  const int j0 = b0 + ((int)blockIdx.x / bk.P) * TWC;
+  if (j0 >= iend) return;  // uniform over the CTA
+  const int nT = (iend + CNB - 1) / CNB;
+  const long long ld = bk.ld[blk];
+  double* Wq = W64 + bk.off[blk];
+  double* C64q = C64 != nullptr ? C64 + bk.off[blk] : nullptr;
+  float* C32q = C32 != nullptr ? C32 + bk.off[blk] : nullptr;
   constexpr int PL = CNB * TKC / TIT;  // L values fetched per thread per chunk
   constexpr int PW = TKC * TWC / TIT;  // W values fetched per thread per chunk
   constexpr int PO = CNB * TWC / TIT;  // outputs per thread per step
@@ -421,7 +432,7 @@ __global__ void __launch_bounds__(TIT) k_tri_inverse(int n, int band, long long 
       for (int m = 0; m < PW; ++m) {
         const int q = t + TIT * m;
         const int kw = k0 + q / TWC, cw = j0 + q % TWC;
-        pw[m] = (kw < i0 && cw < n && cw <= kw) ? W64[(long long)kw * ldc + cw] : 0.0;
+        pw[m] = (kw < i0 && cw < iend && cw <= kw) ? Wq[(long long)(kw - b0) * ld + (cw - b0)] : 0.0;
       }
     };
     double acc[TWC];
@@ -494,33 +505,139 @@ __global__ void __launch_bounds__(TIT) k_tri_inverse(int n, int band, long long 
       const int r = q / TWC, c = q % TWC;
       const int i = i0 + r, col = j0 + c;
       S.Rs[r][c] = wv[p];
-      if (i < n && col < n && col <= i) {
-        W64[(long long)i * ldc + col] = wv[p];
-        if (C64 != nullptr && C64 != W64) C64[(long long)i * ldc + col] = wv[p];
-        if (C32 != nullptr) C32[(long long)i * ldc + col] = (float)wv[p];
+      if (i < iend && col < iend && col <= i) {
+        const long long a = (long long)(i - b0) * ld + (col - b0);
+        Wq[a] = wv[p];
+        if (C64q != nullptr && C64q != Wq) C64q[a] = wv[p];
+        if (C32q != nullptr) C32q[a] = (float)wv[p];
       }
     }
     __syncthreads();
     // transposed copy: rows j0 .. j0+TWC-1 of the upper triangle, columns i0 .. i0+31
-    for (int q = t; q < TWC * CNB; q += TIT) {
-      const int cr = j0 + q / CNB, ic = i0 + q % CNB;
-      if (cr < n && ic < n && ic > cr) {
-        const double v = S.Rs[q % CNB][q / CNB];
-        if (C64 != nullptr) C64[(long long)cr * ldc + ic] = v;
-        if (C32 != nullptr) C32[(long long)cr * ldc + ic] = (float)v;
+    for (int e = t; e < TWC * CNB; e += TIT) {
+      const int cr = j0 + e / CNB, ic = i0 + e % CNB;
+      if (cr < iend && ic < iend && ic > cr) {
+        const double v = S.Rs[e % CNB][e / CNB];
+        const long long a = (long long)(cr - b0) * ld + (ic - b0);
+        if (C64q != nullptr) C64q[a] = v;
+        if (C32q != nullptr) C32q[a] = (float)v;
       }
     }
     __syncthreads();
   }
 }
 
+// ------------------------------------------- couplings between the blocks
+// With the block-bidiagonal L (diagonal blocks L_qq, corners Lc_q = the rows
+// b[q] .. b[q]+band-1 of L over the columns b[q]-band .. b[q]-1), the two
+// triangular solves of K^-1 r become, block by block,
+//   y_q = W_q r_q - G_q y_{q-1}[m_{q-1}-band ..],   G_q = W_q[:, 0:band] Lc_q
+//   z_q = W_q^T y_q - H_q z_{q+1}[0 .. band),       H_q = (Lc_{q+1} W_q[m-band.., :])^T
+// k_couplings forms G_q (q >= 1) and H_q (q < P-1) in FP64 from W64 and L:
+// one CTA per 64 x 32 output tile, 16-wide l chunks staged in shared memory,
+// each thread 2 rows x 4 columns. Lc_q[l][k] is non-zero for l <= k only and
+// W_q is lower triangular, so a tile's l range is clipped to where both are.
+constexpr int GTI = 64, GTK = 32, GTL = 16;
+__global__ void __launch_bounds__(256) k_couplings(int band, long long ldb, const double* __restrict__ L,
+                                                   CoarseBlocks bk, const double* W64, double* C64, float* C32) {
+  __shared__ __align__(16) double As[GTL][GTI + 2];
+  __shared__ __align__(16) double Bs[GTL][GTK + 2];
+  const int q = (int)blockIdx.y >> 1, type = (int)blockIdx.y & 1;  // type 0: G_q, 1: H_q
+  if (q >= bk.P || (type == 0 && q == 0) || (type == 1 && q == bk.P - 1)) return;
+  const int m = bk.b[q + 1] - bk.b[q];
+  const int nkt = (band + GTK - 1) / GTK;
+  const int i0 = ((int)blockIdx.x / nkt) * GTI, k0 = ((int)blockIdx.x % nkt) * GTK;
+  if (i0 >= m) return;
+  const long long ld = bk.ld[q];
+  const double* Wq = W64 + bk.off[q];
+  // rows of L holding the corner: G_q uses block q's, H_q block q+1's
+  const long long cb = type == 0 ? bk.b[q] : bk.b[q + 1];
+  int lo, hi;
+  if (type == 0) {  // l <= k and l <= i
+    lo = 0;
+    hi = min(band, min(k0 + GTK, i0 + GTI));
+  } else {          // l >= k and m-band+l >= i
+    lo = max(k0, i0 - (m - band));
+    lo = max(lo, 0);
+    hi = band;
+  }
+  const int t = threadIdx.x, tx = t & 7, ty = t >> 3;  // columns 4tx.., rows 2ty, 2ty+1
+  double acc[2][4] = {};
+  for (int l0 = lo; l0 < hi; l0 += GTL) {
+    __syncthreads();
+    // A(i, l): G: W_q[i][l]; H: W_q[m-band+l][i]
+#pragma unroll
+    for (int u = 0; u < GTI * GTL / 256; ++u) {
+      const int e = t + 256 * u;
+      int il, ll;
+      if (type == 0) { ll = e % GTL; il = e / GTL; }   // l fastest: a row of W_q
+      else { il = e % GTI; ll = e / GTI; }             // i fastest: a row of W_q
+      const int i = i0 + il, l = l0 + ll;
+      double v = 0.0;
+      if (i < m && l < hi) {
+        if (type == 0) { if (l <= i) v = Wq[(long long)i * ld + l]; }
+        else { const int r = m - band + l; if (r >= i) v = Wq[(long long)r * ld + i]; }
+      }
+      As[ll][il] = v;
+    }
+    // B(l, k): G: Lc_q[l][k] = L[cb+l][cb-band+k]; H: Lc_{q+1}[k][l] = L[cb+k][cb-band+l]
+#pragma unroll
+    for (int u = 0; u < GTK * GTL / 256; ++u) {
+      const int e = t + 256 * u;
+      int kl, ll;
+      if (type == 0) { kl = e % GTK; ll = e / GTK; }
+      else { ll = e % GTL; kl = e / GTL; }
+      const int k = k0 + kl, l = l0 + ll;
+      double v = 0.0;
+      if (k < band && l < hi) {
+        if (type == 0) { if (l <= k) v = L[bidx(cb + l, cb - band + k, band, ldb)]; }
+        else { if (k <= l) v = L[bidx(cb + k, cb - band + l, band, ldb)]; }
+      }
+      Bs[ll][kl] = v;
+    }
+    __syncthreads();
+    const int lend = min(GTL, hi - l0);
+    for (int ll = 0; ll < lend; ++ll) {
+      const double2 a = *reinterpret_cast<const double2*>(&As[ll][2 * ty]);
+      const double2 b01 = *reinterpret_cast<const double2*>(&Bs[ll][4 * tx]);
+      const double2 b23 = *reinterpret_cast<const double2*>(&Bs[ll][4 * tx + 2]);
+      const double b[4] = {b01.x, b01.y, b23.x, b23.y};
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        acc[0][c] = fma(a.x, b[c], acc[0][c]);
+        acc[1][c] = fma(a.y, b[c], acc[1][c]);
+      }
+    }
+  }
+  const int col0 = (type == 0 ? bk.gofs[q] : bk.hofs[q]) + k0 + 4 * tx;
+#pragma unroll
+  for (int r = 0; r < 2; ++r) {
+    const int i = i0 + 2 * ty + r;
+    if (i >= m) continue;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      if (k0 + 4 * tx + c >= band) continue;
+      const long long a = bk.off[q] + (long long)i * ld + col0 + c;
+      if (C64 != nullptr) C64[a] = acc[r][c];
+      if (C32 != nullptr) C32[a] = (float)acc[r][c];
+    }
+  }
+}
+
 // --------------------------------------------------------------- apply
-// z = W^T (W r) over C (W below and on the diagonal, W^T above): pass one
-// y = W r_c (row i reads C[i][0..i]), pass two z_c = W^T y (row j reads
-// C[j][j..n-1]). One warp per row, 16-byte loads (ldc is a multiple of 32
-// elements, so every row starts 16-byte aligned), two loads in flight per
-// lane, FP64 accumulation. The compact right-hand side is gathered once; both
-// passes read the compact vectors (n doubles) through L1.
+// z = K^-1 r block by block: the lower pass for q = 0 .. P-1 forms
+// y_q = W_q r_q - G_q y_{q-1}[tail] (row i reads C_q[i][0..i] and G_q[i]), the
+// upper pass for q = P-1 .. 0 forms z_q = W_q^T y_q - H_q z_{q+1}[head] (row i
+// reads C_q[i][i..m-1] and H_q[i]) and scatters it to the free DoFs. Each row
+// is split over RW warps (interleaved 32-lane chunks of 16-byte loads; row
+// strides and segment starts are multiples of 32 elements, so every segment
+// starts 16-byte aligned), FP64 accumulation, the RW partial sums added
+// through shared memory. With four warps per row one block
+// (about 4 band rows) is a single short wave, so the 2P dependent launches of
+// an apply cost about 5 us each. The compact right-hand side is gathered
+// once; both passes read the compact vectors through L1.
+constexpr int RW = 4;  // warps per row
+
 template <typename T>
 __global__ void k_coarse_gather(int n, long long nfull, const int* __restrict__ free_list, const T* __restrict__ rhs,
                                 double* __restrict__ rc, const KrylovState* st) {
@@ -532,30 +649,32 @@ __global__ void k_coarse_gather(int n, long long nfull, const int* __restrict__ 
   }
 }
 
-// Warp dot product sum_{j in [lo, hi)} Ci[j] v[j] of one row: 16-byte loads
-// from a V-aligned start, four in flight per lane. Every load begins below
-// hi <= n <= ldc at a multiple of V, and ldc is a multiple of 32, so none
-// leaves the row's storage; entries outside [lo, hi) are not used.
+// One warp's share of sum_{j in [lo, hi)} Ci[j] v[j] over a row segment:
+// chunks c = sub, sub+RW, ... of 32 lanes x one 16-byte load, four chunks in
+// flight. Every load begins below hi at a multiple of V and every segment
+// (W_q: m columns, G_q and H_q: band columns) is padded to a multiple of 32,
+// so none leaves its segment; entries outside [lo, hi) are not used.
 template <typename TX>
-__device__ __forceinline__ double row_dot(const TX* __restrict__ Ci, const double* __restrict__ v, int lo, int hi,
-                                          int lane) {
+__device__ __forceinline__ double seg_dot(const TX* __restrict__ Ci, const double* __restrict__ v, int lo, int hi,
+                                          int lane, int sub) {
   constexpr int V = 16 / sizeof(TX);
+  constexpr int STEP = RW * 32 * V;
   constexpr int U = 4;
   double acc = 0.0;
-  int j = (lo / V) * V + lane * V;
-  for (; j + (U - 1) * 32 * V < hi; j += U * 32 * V) {
+  int j = (lo / V) * V + (sub * 32 + lane) * V;
+  for (; j + (U - 1) * STEP < hi; j += U * STEP) {
     TX w[U][V];
 #pragma unroll
-    for (int u = 0; u < U; ++u) *reinterpret_cast<uint4*>(w[u]) = __ldg(reinterpret_cast<const uint4*>(Ci + j + u * 32 * V));
+    for (int u = 0; u < U; ++u) *reinterpret_cast<uint4*>(w[u]) = __ldg(reinterpret_cast<const uint4*>(Ci + j + u * STEP));
 #pragma unroll
     for (int u = 0; u < U; ++u)
 #pragma unroll
       for (int q = 0; q < V; ++q) {
-        const int jj = j + u * 32 * V + q;
+        const int jj = j + u * STEP + q;
         if (jj >= lo && jj < hi) acc += (double)w[u][q] * __ldg(v + jj);
       }
   }
-  for (; j < hi; j += 32 * V) {
+  for (; j < hi; j += STEP) {
     TX w[V];
     *reinterpret_cast<uint4*>(w) = __ldg(reinterpret_cast<const uint4*>(Ci + j));
 #pragma unroll
@@ -564,33 +683,62 @@ __device__ __forceinline__ double row_dot(const TX* __restrict__ Ci, const doubl
       if (jj >= lo && jj < hi) acc += (double)w[q] * __ldg(v + jj);
     }
   }
-  return warp_sum(acc);
+  return acc;
 }
 
-// pass one: y = W r_c (row i reads C[i][0..i])
+// Sum of the RW warp partials of each row of the CTA (every thread calls it).
+__device__ __forceinline__ double row_sum(double acc, int warp, int lane) {
+  __shared__ double part[8];
+  acc = warp_sum(acc);
+  if (lane == 0) part[warp] = acc;
+  __syncthreads();
+  double t = 0.0;
+  if (warp % RW == 0)
+#pragma unroll
+    for (int k = 0; k < RW; ++k) t += part[warp + k];
+  return t;
+}
+
+// pass one, block q (rows b0 .. b0+m-1): y_q = W_q r_q - G_q y_{q-1}[m_{q-1}-band ..]
 template <typename TX>
-__global__ void __launch_bounds__(256) k_coarse_lower(int n, long long ldc, const TX* __restrict__ C,
-                                                      const double* __restrict__ rc, double* __restrict__ y,
-                                                      const KrylovState* st) {
-  if (st != nullptr && st->done) return;
-  const int row = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
-  if (row >= n) return;
-  const double acc = row_dot(C + (long long)row * ldc, rc, 0, row + 1, lane);
-  if (lane == 0) y[row] = acc;
+__global__ void __launch_bounds__(256) k_coarse_lower(int m, int b0, long long ld, int gofs, int band, int prev,
+                                                      const TX* __restrict__ Cq, const double* __restrict__ rc,
+                                                      double* y, const KrylovState* st) {
+  if (st != nullptr && st->done) return;  // uniform over the grid
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int row = (int)blockIdx.x * (8 / RW) + warp / RW, sub = warp % RW;
+  const bool live = row < m;
+  double acc = 0.0;
+  if (live) {
+    const TX* Ci = Cq + (long long)row * ld;
+    acc = seg_dot(Ci, rc + b0, 0, row + 1, lane, sub);
+    if (prev) acc -= seg_dot(Ci + gofs, y + (b0 - band), 0, band, lane, sub);
+  }
+  acc = row_sum(acc, warp, lane);
+  if (live && sub == 0 && lane == 0) y[b0 + row] = acc;
 }
 
-// pass two: z_c = W^T y (row j reads C[j][j..n-1]), scattered to the free DoFs
+// pass two, block q: z_q = W_q^T y_q - H_q z_{q+1}[0 .. band), kept compact in
+// z and scattered to the free DoFs of x
 template <typename T, typename TX>
-__global__ void __launch_bounds__(256) k_coarse_upper(int n, long long nfull, long long ldc, const TX* __restrict__ C,
-                                                      const int* __restrict__ free_list,
-                                                      const double* __restrict__ y, T* __restrict__ x,
-                                                      const KrylovState* st) {
-  if (st != nullptr && st->done) return;
-  const int row = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
-  if (row >= n) return;
-  const double acc = row_dot(C + (long long)row * ldc, y, row, n, lane);
-  if (lane == 0) {
-    const int f = free_list[row];
+__global__ void __launch_bounds__(256) k_coarse_upper(int m, int b0, long long ld, int hofs, int band, int next,
+                                                      long long nfull, const TX* __restrict__ Cq,
+                                                      const int* __restrict__ free_list, const double* y, double* z,
+                                                      T* __restrict__ x, const KrylovState* st) {
+  if (st != nullptr && st->done) return;  // uniform over the grid
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int row = (int)blockIdx.x * (8 / RW) + warp / RW, sub = warp % RW;
+  const bool live = row < m;
+  double acc = 0.0;
+  if (live) {
+    const TX* Ci = Cq + (long long)row * ld;
+    acc = seg_dot(Ci, y + b0, row, m, lane, sub);
+    if (next) acc -= seg_dot(Ci + hofs, z + (b0 + m), 0, band, lane, sub);
+  }
+  acc = row_sum(acc, warp, lane);
+  if (live && sub == 0 && lane == 0) {
+    z[b0 + row] = acc;
+    const int f = free_list[b0 + row];
     if (topo_in_range(f, nfull)) x[f] = (T)acc;
   }
 }
@@ -618,9 +766,35 @@ void coarsest_alloc(CoarsestFactor& f, const CoarsestPlan& p, int band, bool f64
   f.L = (double*)A(nbs * sizeof(double));
   f.Dinv = (double*)A((size_t)std::max(p.nt, 1) * cst::CNB * cst::CNB * sizeof(double));
   f.Lnext = (double*)A(2 * (size_t)(cst::CNB * (cst::CNB + 1) + cst::CNB) * sizeof(double));
-  f.ldc = ((long long)n + 31) / 32 * 32;
-  f.W64 = (double*)A((size_t)n * f.ldc * sizeof(double));
-  f.C = f64 ? (void*)f.W64 : A((size_t)n * f.ldc * sizeof(float));
+  // diagonal blocks of W: at least max(4 band, 512) rows each (every block at
+  // least `band` rows), boundaries on 32-row panels
+  CoarseBlocks& bk = f.blk;
+  int P = std::max(1, std::min(COARSE_MAXB, n / std::max(4 * band, 512)));
+  for (;;) {
+    bk.P = P;
+    bk.b[0] = 0;
+    for (int q = 1; q < P; ++q) bk.b[q] = (int)((long long)q * n / P / cst::CNB * cst::CNB);
+    bk.b[P] = n;
+    bool ok = true;
+    for (int q = 0; q < P; ++q) ok = ok && bk.b[q + 1] - bk.b[q] >= std::max(band, 1);
+    if (ok || P == 1) break;
+    --P;
+  }
+  const long long bandp = ((long long)band + 31) / 32 * 32;
+  long long off = 0;
+  int maxm = 0;
+  for (int q = 0; q < bk.P; ++q) {
+    const int m = bk.b[q + 1] - bk.b[q];
+    maxm = std::max(maxm, m);
+    bk.gofs[q] = (m + 31) / 32 * 32;
+    bk.hofs[q] = (int)(bk.gofs[q] + bandp);
+    bk.ld[q] = bk.gofs[q] + (bk.P > 1 ? 2 * bandp : 0);
+    bk.off[q] = off;
+    off += (long long)m * bk.ld[q];
+  }
+  f.strips_per_block = (maxm + cst::TWC - 1) / cst::TWC;
+  f.W64 = (double*)A((size_t)off * sizeof(double));
+  f.C = f64 ? (void*)f.W64 : A((size_t)off * sizeof(float));
   f.flag = (int*)A(sizeof(int) * 4);
   f.bar = (unsigned*)A(sizeof(unsigned) * 4);
   f.err = f.flag + 1;
@@ -633,7 +807,6 @@ void coarsest_alloc(CoarsestFactor& f, const CoarsestPlan& p, int band, bool f64
   TOPO_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cst::k_band_chol, 256, sizeof(cst::CholSmem)));
   const int tiles_max = ((band + cst::CNB - 1) / cst::CNB) * ((band + cst::CNB - 1) / cst::CNB + 1) / 2;
   f.chol_grid = std::max(1, std::min(std::min(nsm * std::max(per_sm, 1), nsm), std::max(tiles_max, 1)));
-  f.nsm = nsm;
   TOPO_CUDA_CHECK(cudaFuncSetAttribute(cst::k_tri_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)sizeof(cst::TriSmem)));
   f.plan = p;
@@ -682,10 +855,20 @@ void coarsest_factor(CoarsestFactor& f, cudaStream_t s) {
   }
   cst::k_diag_inverse<<<p.nt, cst::CNB, 0, s>>>(n, f.band, f.ldb, f.L, f.Dinv);
   TOPO_LAUNCH_CHECK();
-  cst::k_tri_inverse<<<(n + cst::TWC - 1) / cst::TWC, cst::TIT, sizeof(cst::TriSmem), s>>>(
-      n, f.band, f.ldb, f.L, f.Dinv, f.W64, f.ldc, f.f64 ? f.W64 : nullptr, f.f64 ? nullptr : (float*)f.C,
-      (n + cst::TWC - 1) / cst::TWC >= 3 * f.nsm ? f.nsm : 0);
+  const CoarseBlocks& bk = f.blk;
+  double* C64 = f.f64 ? f.W64 : nullptr;
+  float* C32 = f.f64 ? nullptr : (float*)f.C;
+  cst::k_tri_inverse<<<(unsigned)(bk.P * f.strips_per_block), cst::TIT, sizeof(cst::TriSmem), s>>>(
+      n, f.band, f.ldb, f.L, f.Dinv, bk, f.W64, C64, C32);
   TOPO_LAUNCH_CHECK();
+  if (bk.P > 1) {
+    int maxm = 0;
+    for (int q = 0; q < bk.P; ++q) maxm = std::max(maxm, bk.b[q + 1] - bk.b[q]);
+    const int nkt = (f.band + cst::GTK - 1) / cst::GTK;
+    const dim3 grid((unsigned)(((maxm + cst::GTI - 1) / cst::GTI) * nkt), (unsigned)(2 * bk.P));
+    cst::k_couplings<<<grid, 256, 0, s>>>(f.band, f.ldb, f.L, bk, f.W64, C64, C32);
+    TOPO_LAUNCH_CHECK();
+  }
 }
 
 // Returns the non-positive-pivot flag (1) or a barrier timeout (< 0).
@@ -697,41 +880,46 @@ int coarsest_status(CoarsestFactor& f, cudaStream_t s) {
   return h[0] ? 1 : 0;
 }
 
-// work: 2n doubles (y, then the compact right-hand side).
-void coarsest_apply(const CoarsestFactor& f, bool vec64, const void* rhs, double* work, void* x, const KrylovState* st,
-                    cudaStream_t s) {
+// work: 2n doubles (y, then the compact right-hand side, overwritten by the
+// compact solution in the second pass).
+template <typename T, typename TX>
+static void apply_blocks(const CoarsestFactor& f, const T* rhs, double* work, T* x, const KrylovState* st,
+                         cudaStream_t s) {
   const CoarsestPlan& p = f.plan;
+  const CoarseBlocks& bk = f.blk;
   const int n = p.n;
-  if (n == 0) return;
-  const int wpb = 8;
-  const unsigned nb = (unsigned)((n + wpb - 1) / wpb);
-  const unsigned ng = (unsigned)((n + 255) / 256);
+  constexpr int rpb = 8 / cst::RW;  // rows per 256-thread CTA
   double* y = work;
   double* rc = work + n;
+  const TX* C = (const TX*)f.C;
+  cst::k_coarse_gather<T><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, p.nfull, f.d_free, rhs, rc, st);
+  TOPO_LAUNCH_CHECK();
+  for (int q = 0; q < bk.P; ++q) {
+    const int m = bk.b[q + 1] - bk.b[q];
+    cst::k_coarse_lower<TX><<<(unsigned)((m + rpb - 1) / rpb), 256, 0, s>>>(
+        m, bk.b[q], bk.ld[q], bk.gofs[q], f.band, (int)(q > 0), C + bk.off[q], rc, y, st);
+    TOPO_LAUNCH_CHECK();
+  }
+  for (int q = bk.P - 1; q >= 0; --q) {
+    const int m = bk.b[q + 1] - bk.b[q];
+    cst::k_coarse_upper<T, TX><<<(unsigned)((m + rpb - 1) / rpb), 256, 0, s>>>(
+        m, bk.b[q], bk.ld[q], bk.hofs[q], f.band, (int)(q < bk.P - 1), p.nfull, C + bk.off[q], f.d_free, y, rc, x,
+        st);
+    TOPO_LAUNCH_CHECK();
+  }
+}
+
+void coarsest_apply(const CoarsestFactor& f, bool vec64, const void* rhs, double* work, void* x, const KrylovState* st,
+                    cudaStream_t s) {
+  if (f.plan.n == 0) return;
   if (vec64) {
     if (!f.f64) throw std::runtime_error("coarsest apply: FP64 vectors need the FP64 inverse");
-    cst::k_coarse_gather<double><<<ng, 256, 0, s>>>(n, p.nfull, f.d_free, (const double*)rhs, rc, st);
-    TOPO_LAUNCH_CHECK();
-    cst::k_coarse_lower<double><<<nb, 32 * wpb, 0, s>>>(n, f.ldc, (const double*)f.C, rc, y, st);
-    TOPO_LAUNCH_CHECK();
-    cst::k_coarse_upper<double, double><<<nb, 32 * wpb, 0, s>>>(n, p.nfull, f.ldc, (const double*)f.C, f.d_free, y,
-                                                                (double*)x, st);
+    apply_blocks<double, double>(f, (const double*)rhs, work, (double*)x, st, s);
+  } else if (f.f64) {
+    apply_blocks<float, double>(f, (const float*)rhs, work, (float*)x, st, s);
   } else {
-    cst::k_coarse_gather<float><<<ng, 256, 0, s>>>(n, p.nfull, f.d_free, (const float*)rhs, rc, st);
-    TOPO_LAUNCH_CHECK();
-    if (f.f64) {
-      cst::k_coarse_lower<double><<<nb, 32 * wpb, 0, s>>>(n, f.ldc, (const double*)f.C, rc, y, st);
-      TOPO_LAUNCH_CHECK();
-      cst::k_coarse_upper<float, double><<<nb, 32 * wpb, 0, s>>>(n, p.nfull, f.ldc, (const double*)f.C, f.d_free, y,
-                                                                 (float*)x, st);
-    } else {
-      cst::k_coarse_lower<float><<<nb, 32 * wpb, 0, s>>>(n, f.ldc, (const float*)f.C, rc, y, st);
-      TOPO_LAUNCH_CHECK();
-      cst::k_coarse_upper<float, float><<<nb, 32 * wpb, 0, s>>>(n, p.nfull, f.ldc, (const float*)f.C, f.d_free, y,
-                                                                (float*)x, st);
-    }
+    apply_blocks<float, float>(f, (const float*)rhs, work, (float*)x, st, s);
   }
-  TOPO_LAUNCH_CHECK();
 }
 
 TOPO_BOUNDS_READER(bounds_flag_coarsest)

@@ -249,11 +249,27 @@ void restrict_vec(bool vec64, const Grid& fine, const Grid& coarse, const void* 
 void prolong_add(bool vec64, const Grid& fine, const Grid& coarse, const void* ec, const uint8_t* mf,
                  void* xf, void* e_out, const KrylovState* st, cudaStream_t s);
 // coarsest level (coarsest.cu): band Cholesky of the free-DoF operator and
-// block sweeps over its x-plane blocks. Compact DoF i -> full DoF free[i].
+// the inverses of its diagonal blocks. Compact DoF i -> full DoF free[i].
 struct CoarsestPlan {
   int n = 0;                                // free DoFs (compact rows)
   int nt = 0;                               // 32-row blocks
   long long nfull = 0;                      // DoFs of the full coarsest-level vectors
+};
+// Diagonal blocks of the coarsest factor: rows b[q] .. b[q+1]-1 (boundaries
+// multiples of 32, every block at least `band` rows, so L couples block q+1
+// to block q only through the band x band corner L[b[q+1]+k][b[q+1]-band+l],
+// l >= k). Block q of the apply matrix starts at element off[q], row stride
+// ld[q]: columns 0 .. m-1 hold W_q = L_qq^-1 (lower) and W_q^T (strict upper),
+// columns gofs .. gofs+band-1 G_q = W_q Lc_q, columns hofs .. hofs+band-1
+// H_q = (Lc_{q+1} W_q[m-band .. m-1, :])^T.
+constexpr int COARSE_MAXB = 8;
+struct CoarseBlocks {
+  int P = 1;
+  int b[COARSE_MAXB + 1] = {};
+  long long off[COARSE_MAXB] = {};
+  long long ld[COARSE_MAXB] = {};
+  int gofs[COARSE_MAXB] = {};
+  int hofs[COARSE_MAXB] = {};
 };
 struct CoarsestFactor {
   CoarsestPlan plan;
@@ -263,14 +279,14 @@ struct CoarsestFactor {
   double *A = nullptr, *L = nullptr;        // band storage (n x (band+1)): operator, factor
   double* Dinv = nullptr;                   // inverses of the 32x32 diagonal blocks of L
   double* Lnext = nullptr;                  // look-ahead: the next panel's factored block (two slots)
-  double* W64 = nullptr;                    // W = L^-1 (lower triangle, row stride ldc)
-  void* C = nullptr;                        // apply matrix: W below, W^T above (W64 itself in FP64)
-  long long ldc = 0;
+  CoarseBlocks blk;                         // diagonal blocks of W and the apply matrix
+  double* W64 = nullptr;                    // per block: W_q (lower), in FP64 also W_q^T, G_q, H_q
+  void* C = nullptr;                        // apply matrix in the apply precision (W64 itself in FP64)
   int* flag = nullptr;                      // [0] non-positive pivot, [1] barrier timeout
   int* err = nullptr;
   unsigned* bar = nullptr;
   int chol_grid = 1;
-  int nsm = 0;                              // SMs of the device (W strip placement)
+  int strips_per_block = 0;                 // 16-column W strips of the largest block
   const int* d_free = nullptr;
   int kind = 0;                             // 0 none, 1 Cholesky, 2 Cholesky of K + eps I
 };
