@@ -597,6 +597,8 @@ void do_setup(topo_ctx* c, const double* E, cudaStream_t s) {
   TOPO_CUDA_CHECK(cudaEventRecord(c->ev_ph[2], s));
   TOPO_CUDA_CHECK(cudaEventRecord(c->ev_ph[3], s));
   TOPO_CUDA_CHECK(cudaEventRecord(c->ev_ph[4], s));
+  // the side stream starts from here, beside the factorisation queued next
+  TOPO_CUDA_CHECK(cudaEventRecord(c->C.ev_rap, s));
   // coarsest: FP64 band Cholesky + W = L^-1, with the reference's eps*I
   // retry (multigrid_v4.py:778-811)
   bool launched_cur = false;
@@ -630,7 +632,6 @@ void do_setup(topo_ctx* c, const double* E, cudaStream_t s) {
   }
   {
     cudaStream_t t = c->C.side;
-    TOPO_CUDA_CHECK(cudaEventRecord(c->C.ev_rap, s));
     TOPO_CUDA_CHECK(cudaStreamWaitEvent(t, c->C.ev_rap, 0));
     for (int l = 1; l < c->n_levels - 1; ++l) {
       Level& Lv = c->L[l];
