@@ -45,16 +45,24 @@ FALLBACK_PEAKS = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
 
 def traffic_for(name: str):
     """DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of
-    a kernel from its committed ncu summary, used only when that capture was
-    taken with the library being run (same SHA-256), else None."""
+    a kernel from its committed ncu summary, used only while the sources that
+    compile into that kernel (listed in the summary, with the build flags'
+    file) are byte for byte the ones it was captured from, else None. The
+    sources, not the library, are hashed: nvcc builds of the same source
+    differ in embedded module identifiers."""
     import hashlib
 
     f = ROOT / "profiles" / f"{name}_traffic.json"
-    lib = ROOT / "topogpu_b200" / "libtopo_b200.so"
-    if not f.exists() or not lib.exists():
+    if not f.exists():
         return None
     d = json.loads(f.read_text())
-    if d.get("lib_sha256") != hashlib.sha256(lib.read_bytes()).hexdigest():
+    srcs = d.get("sources")
+    if not srcs or any(not (ROOT / p).exists() for p in srcs):
+        return None
+    h = hashlib.sha256()
+    for p in srcs:
+        h.update((ROOT / p).read_bytes())
+    if d.get("src_sha256") != h.hexdigest():
         return None
     return d.get("bytes_per_launch")
 
