@@ -599,8 +599,8 @@ void do_setup(topo_ctx* c, const double* E, cudaStream_t s) {
   TOPO_CUDA_CHECK(cudaEventRecord(c->ev_ph[4], s));
   // the side stream starts from here, beside the factorisation queued next
   TOPO_CUDA_CHECK(cudaEventRecord(c->C.ev_rap, s));
-  // coarsest: FP64 band Cholesky + W = L^-1, with the reference's eps*I
-  // retry (multigrid_v4.py:778-811)
+  // coarsest: FP64 band Cholesky + diagonal-block inverses, with the
+  // reference's eps*I retry (multigrid_v4.py:778-811)
   bool launched_cur = false;
   if (c->n_levels > 1 && c->C.n > 0) {
     Level& Lc = c->L[c->n_levels - 1];
