@@ -303,10 +303,12 @@ int topo_field_stats(topo_ctx* ctx, const double* x, long long n, double* out_ho
 int topo_gmg_info(topo_ctx* ctx, long long* n_free, double* lambda_max, int* coarse_kind);
 /* Device time (ms) of the phases of the last topo_gmg_setup: ms[0] fine
  * diagonal and lambda_max check, ms[1] coarse stencils (level-1 Galerkin,
- * R.A.P, Jacobi, lambda, conversions), ms[2] copy of the coarsest stencil,
- * ms[3] coarsest factorisation (assembly, banded Cholesky and W = L^-1, one
- * graph; 0 when it runs in the background under topo_set_coarse_lag),
- * ms[4] pivot check and eps*I retry. Diagnostic of GalerkinMatFreeGMG.setup
+ * R.A.P), ms[2] copy of the coarsest stencil, ms[3] coarsest factorisation
+ * (assembly, banded Cholesky, inverses of its diagonal blocks and their
+ * couplings, one graph; the coarse levels' Jacobi diagonals, lambda and
+ * stencil conversions run beside it on a second stream; 0 when it runs in
+ * the background under topo_set_coarse_lag), ms[4] the join of that stream,
+ * pivot check and eps*I retry. Diagnostic of GalerkinMatFreeGMG.setup
  * (src/gpu_fem/multigrid_v4.py:657-811), which the reference times only as a
  * whole in SolverV4.last_timing (solver_v4.py:231-267). */
 int topo_setup_phases(topo_ctx* ctx, double* ms);
