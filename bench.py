@@ -425,32 +425,45 @@ def reference_arm(args, rank):
     """The reference's algorithm on the host cores (the CPU oracle: the
     reference is Python on CuPy, which is not installed, so it cannot run
     on the GPU box itself). Each step is one SIMP iteration of the REF_SAMPLE
-    mesh (after the warm-up iterations of the same run), carried to
-    160x80x80 linearly in the element count."""
+    mesh, carried to 160x80x80 linearly in the element count. The run
+    restarts from the uniform density every two iterations (construction not
+    timed), so every step is iteration 1 or 2: the regime in which the
+    linear scaling was checked against a direct 160x80x80 run, and a bounded
+    cost per step (later iterations of the oracle's FP32 smoother need many
+    more PCG iterations on this mesh: 60 and 162 at iterations 3 and 4)."""
     if rank != 0:
         return 0
     os.environ.setdefault("OMP_NUM_THREADS", str(len(os.sched_getaffinity(0))))
     from oracle import fem, simp
 
     bc = fem.cantilever_bc(REF_SAMPLE)
-    s = simp.FilteredSIMP(REF_SAMPLE, bc, 0.30, 2.0, move=0.2, n_levels=4, fine_prec="fp32", fine_degree=3, tol=1e-5,
-                          maxiter=800)
+    state = {"s": None, "k": 0}
+
+    def one_iteration():
+        if state["k"] % 2 == 0:
+            state["s"] = simp.FilteredSIMP(REF_SAMPLE, bc, 0.30, 2.0, move=0.2, n_levels=4, fine_prec="fp32",
+                                           fine_degree=3, tol=1e-5, maxiter=800)
+        state["k"] += 1
+        t0 = time.perf_counter()
+        state["s"].step()
+        return time.perf_counter() - t0, state["s"].state.last_iters
+
     for _ in range(args.warmup):
-        s.step()
+        one_iteration()
     times, its = [], []
     for _ in range(args.steps):
-        t0 = time.perf_counter()
-        s.step()
-        times.append(time.perf_counter() - t0)
-        its.append(s.state.last_iters)
+        t, it = one_iteration()
+        times.append(t)
+        its.append(it)
     ms = scale_to_full(statistics.mean(times)) * 1e3
     value = 1e3 / ms
     cores = len(os.sched_getaffinity(0))
-    sample = (f"SIMP iterations {args.warmup + 1}..{args.warmup + args.steps} of the CPU oracle (restated reference "
-              f"SolverV4 GMG-PCG: FP64 PCG, FP32 Chebyshev smoother deg 3, 4 levels, rtol 1e-5, filter rmin 2.0) on "
-              f"{'x'.join(map(str, REF_SAMPLE))} ({int(np.prod(REF_SAMPLE))} hex, PCG its {its}, "
-              f"{statistics.mean(times):.2f} s/it), carried to 1,024,000 hex linearly in the element count "
-              f"(checked on 8 cores against a direct 160x80x80 run: 154.5 s predicted, 162.8 s measured)")
+    sample = (f"{args.steps} SIMP iterations of the CPU oracle (restated reference SolverV4 GMG-PCG: FP64 PCG, FP32 "
+              f"Chebyshev smoother deg 3, 4 levels, rtol 1e-5, filter rmin 2.0) on {'x'.join(map(str, REF_SAMPLE))} "
+              f"({int(np.prod(REF_SAMPLE))} hex), each iteration 1 or 2 of a run restarted from the uniform density "
+              f"every two (PCG its {its}, {statistics.mean(times):.2f} s/it), carried to 1,024,000 hex linearly in "
+              f"the element count (checked on 8 cores against a direct 160x80x80 run of iterations 1-2: 154.5 s "
+              f"predicted, 162.8 s measured)")
     line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
             "sample_ms_per_step": statistics.mean(times) * 1e3, "higher_is_better": True,
