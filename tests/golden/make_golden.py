@@ -16,11 +16,11 @@ reference. Every array is produced by reference code paths:
   galerkin.npz     GalerkinMatFreeGMG.setup: K1 (level-1 Galerkin), K2, K3 (R.A.P),
                    lambda estimates, one V-cycle apply    (multigrid_v4.py)
   krylov.npz       _cupy_pcg and _cupy_fgmres with the GMG preconditioner
-  solverv4.npz     SolverV4 + topogpu._oc_update, 3 SIMP iterations, config-0
+  solverv4.npz     SolverV4 + topogpu._oc_update, 3 SIMP iterations, 24x12x6
                    cantilever (FP64 and FP32 smoothers)
   oc.npz           topogpu.solver._oc_update on seeded inputs
   filter.npz       _build_density_filter (rmin 1.5, 2.0), DensityFilter.matrix
-  run_simp.npz     run_simp config 0 (rmin 1.5, move 0.2, no Heaviside)
+  run_simp.npz     run_simp on the 24x12x6 cantilever (rmin 1.5, move 0.2, no Heaviside)
   run_simp_heaviside.npz  run_simp on the same mesh with Heaviside
                    projection at beta 1 (the SIMPParams default) and beta 8
   wcycle.npz       GalerkinMatFreeGMG(cycle_type="w").apply and PCG on the
@@ -31,7 +31,7 @@ reference. Every array is produced by reference code paths:
   run_simp_resume.npz  run_simp on the 3-D preset interrupted after 4 of 7
                    iterations (checkpoint_every 2) and resumed: both legs
   ckpt_24x12x6_cantilever.{npz,json}  the checkpoint run_simp writes after
-                   iteration 2 of config 0 (checkpoint_every 1)
+                   iteration 2 of that 24x12x6 run (checkpoint_every 1)
 
 ``python make_golden.py [REF_ROOT] [--only heaviside|checkpoint|wcycle|control|resume]``
 regenerates all fixtures, or only the named group.
@@ -173,7 +173,7 @@ def main(ref_root: str) -> None:
         d[f"fgmres_it_{tag}"] = np.array(it2)
     np.savez_compressed(HERE / "galerkin.npz", **d)
 
-    # ---- SolverV4 + OC, config-0 cantilever ------------------------------
+    # ---- SolverV4 + OC, 24x12x6 cantilever --------------------------------
     d = {}
     nel = (24, 12, 6)
     edof = _edof_table_3d(*nel)
@@ -223,7 +223,7 @@ def main(ref_root: str) -> None:
     d["dense_322_r1.5"] = tg.DensityFilter((3, 2, 2), radius=1.5).matrix()
     np.savez_compressed(HERE / "filter.npz", **d)
 
-    # ---- run_simp config 0 ---------------------------------------------------
+    # ---- run_simp, 24x12x6 cantilever --------------------------------------
     nel = (24, 12, 6)
     fixed, free, F, ndof = cantilever_bc(nel)
     params = SIMPParams(nelx=24, nely=12, nelz=6, volfrac=0.3, rmin=1.5, move=0.2, max_iter=3, min_iter=3,

@@ -23,7 +23,7 @@ def test_batched_uneven_meshes_match_single_fp64(cuda_dev):
     tune = bs.autotune(rhos)
     res = bs.solve(rhos)
     s = summarize(res)
-    print("config 4b autotune:", tune["choice"], "->", {k: (round(v, 2) if isinstance(v, float) else v)
+    print("64 uneven meshes, autotune:", tune["choice"], "->", {k: (round(v, 2) if isinstance(v, float) else v)
                                                           for k, v in s.items()})
     assert s["all_converged"] and s["mean_pcg_iters"] > 0
     ref = BatchSolver(meshes, precision="fp64", tol=1e-10)

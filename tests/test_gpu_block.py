@@ -90,7 +90,7 @@ def test_block_pcg_config4a_mixed_vs_fp64(cuda_dev):
     c64, cm = np.array(out["fp64"][0]), np.array(out["mixed"][0])
     assert out["fp64"][3] and out["mixed"][3]
     rel = np.abs(cm - c64) / np.abs(c64)
-    print(f"config 4a: block PCG fp64 {out['fp64'][1]} it / {out['fp64'][2] * 1e3:.1f} ms, "
+    print(f"8 load cases: block PCG fp64 {out['fp64'][1]} it / {out['fp64'][2] * 1e3:.1f} ms, "
           f"mixed {out['mixed'][1]} it / {out['mixed'][2] * 1e3:.1f} ms, "
           f"8 single mixed solves {out['single'][0]} it / {out['single'][1] * 1e3:.1f} ms; "
           f"max compliance rel err {rel.max():.2e}")

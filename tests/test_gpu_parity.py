@@ -340,8 +340,8 @@ def test_simp_solverv4_config0_fp64(cuda_dev):
 @pytest.mark.parametrize("precision,tol", [("fp64", 1e-5), ("fp32", 1e-4), ("mixed", 1e-4)])
 def test_reduced_precision_compliance_vs_fp64_oracle(cuda_dev, precision, tol):
     """Compliance of each precision mode against the direct FP64 solve on a
-    high-contrast random density (config-3 input): within 1e-4 relative at
-    rtol 1e-5. The Chebyshev smoother keeps every mode within
+    high-contrast random density (48x24x24, rho ~ U[0.05, 1] filtered with
+    rmin 1.5): within 1e-4 relative at rtol 1e-5, the required bar. The Chebyshev smoother keeps every mode within
     a few tens of PCG iterations (the reference recurrence needs 93-140 in
     FP64 on this input and does not converge in FP32)."""
     from topogpu_b200.state import StateSolver
@@ -371,7 +371,7 @@ def test_mixed_solution_at_size_checked_by_oracle_operator(cuda_dev):
     (rtol 1e-8) are checked with the oracle's own matrix-free FP64 K.u, so the
     bar does not rest on this library's FP64 path: true relative residual
     <= 5e-5 (mixed) and <= 1e-7 (FP64) on the free DoFs, and the mixed
-    compliance within 1e-4 of the FP64 one. A converged
+    compliance within 1e-4 of the FP64 one (the required bar). A converged
     oracle solve at this size takes minutes on the host, so the oracle
     checks the residual instead."""
     from topogpu_b200.state import StateSolver
